@@ -1,0 +1,66 @@
+// Oracle: CPU restatement of the VMC sampling + SR hot path of AtelierArith/mvmc-rs.
+//
+// TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path: tests/,
+// __graft_entry__.smoke() and bench.py's cpu_baseline leg (and `bench.py --impl
+// reference`) are the only callers. The product (mvmc-rs_b200/) never links it.
+//
+// Parity is pinned against the reference's own C-1.4.0 fixtures, read as text:
+//   * SFMT19937 first words per seed (crates/sfmt19937/tests/golden_vs_c.rs)
+//   * every saved configuration, counter, draw count and the next 624 SFMT words of a
+//     native C sampler run (tests/fixtures/native_c_physcal_181/hubbard_chain_real)
+//   * step-1 SR operands E, HO, <O>, <O^2>, last O (tests/fixtures/c_order_sr_operands)
+//   * pfapack identities on tests/fixtures/pfapack/real_n*.orig.txt
+#pragma once
+#include <cstdint>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// SFMT19937: first `count` gen_rand32 words after init_gen_rand(seed).
+void oracle_sfmt_words(uint32_t seed, int count, uint32_t* out);
+
+// Batched Pfaffian + inverse of skew-symmetric planes (column-major, back to back).
+// Mirrors PfaffianStages::pfaffian_inverse_batch: `inv` receives the true X^-1,
+// `status[p]` = 0 ok, k > 0 the 1-based zero-pivot row, -1 non-finite Pfaffian.
+void oracle_pfinv_batch(const double* x, int n, int planes, double* pf, double* inv, int* status);
+
+// Full optimisation run (vmc_para_opt) with W independent chains seeded RndSeed + w.
+// Writes zvo_out.dat / zvo_var.dat / zvo_SRinfo.dat / zqp_*opt.dat into out_dir.
+// nsteps <= 0 keeps NSROptItrStep. Returns 0 on success, nonzero on failure; the
+// message is copied to `err` (size err_len).
+int oracle_run_opt(const char* namelist, const char* initial_def, const char* out_dir,
+                   int walkers, int nsteps, long long seed_override, char* err, int err_len);
+
+// One optimisation step's SR operands before the solve (C NSROptItrStep = 1), for the
+// step-1 fixtures. Overrides: NSRCG=cg, NStore=store, RndSeed=seed. Outputs (sizes
+// sr_size = 1 + NPara): energy[1], ho[sr_size], oo[2*sr_size] (mean then diagonal),
+// o_last[sr_size].
+int oracle_step1_operands(const char* namelist, int cg, int store, long long seed,
+                          double* energy, double* ho, double* oo, double* o_last, int sr_size,
+                          char* err, int err_len);
+
+// PhysCal sampling with fixed parameters from zqp_opt.dat (vmc_phys_cal): records every
+// saved configuration of NDataQtySmp sample blocks. Output arrays are sized by the
+// caller: ele_idx[blocks*NS*nsize], ele_cfg[blocks*NS*2Ns], ele_num[same],
+// proj_cnt[blocks*NS*NProj], counters[blocks*6], draws[blocks], next624[blocks*624],
+// energies[blocks*2] (<E>, <E^2> of each block's measurement).
+int oracle_physcal_samples(const char* namelist, const char* zqp_opt, long long seed,
+                           int64_t* ele_idx, int64_t* ele_cfg, int64_t* ele_num,
+                           int64_t* proj_cnt, int64_t* counters, int64_t* draws,
+                           uint32_t* next624, double* energies, char* err, int err_len);
+
+// SR-CG on fixed operands (SampledSrOperator::solve_with_product): samples are
+// [samples][n]; returns the C status (iterations, or -(iter+1)). z_apply (optional)
+// receives S·g.
+int oracle_cg_fixed(int n, int samples, const double* mean, const double* diag, const double* smp,
+                    const double* g, double inv_w, double shift, double tol, int max_iter,
+                    int diag_scale, double* x_out, double* z_apply);
+
+// Model dimensions for buffer sizing: [nsite, ne, nqp, nproj, npara, nvmc_sample,
+// data_qty_smp, n_orb].
+int oracle_model_dims(const char* namelist, int* dims, char* err, int err_len);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,107 @@
+"""ctypes loader for the oracle (test infrastructure: the CPU checker of the CUDA path)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+        _LIB = ctypes.CDLL(path)
+    return _LIB
+
+
+def ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def err_buf():
+    return ctypes.create_string_buffer(1024)
+
+
+def model_dims(namelist):
+    dims = (ctypes.c_int * 8)()
+    err = err_buf()
+    if lib().oracle_model_dims(namelist.encode(), dims, err, 1024) != 0:
+        raise RuntimeError(err.value.decode())
+    keys = ["nsite", "ne", "nqp", "nproj", "npara", "nvmc_sample", "data_qty_smp", "n_orb"]
+    return dict(zip(keys, list(dims)))
+
+
+def sfmt_words(seed, count):
+    out = (ctypes.c_uint32 * count)()
+    lib().oracle_sfmt_words(ctypes.c_uint32(seed), count, out)
+    return list(out)
+
+
+def pfinv_batch(x_colmajor, n, planes):
+    x = np.ascontiguousarray(x_colmajor, dtype=np.float64)
+    pf = np.zeros(planes)
+    inv = np.zeros(planes * n * n)
+    st = np.zeros(planes, dtype=np.int32)
+    lib().oracle_pfinv_batch(ptr(x), n, planes, ptr(pf), ptr(inv), ptr(st))
+    return pf, inv, st
+
+
+def physcal_samples(namelist, zqp, seed):
+    d = model_dims(namelist)
+    n, ns2, npj = 2 * d["ne"], 2 * d["nsite"], d["nproj"]
+    b, S = d["data_qty_smp"], d["nvmc_sample"]
+    out = dict(
+        ele_idx=np.zeros(b * S * n, np.int64), ele_cfg=np.zeros(b * S * ns2, np.int64),
+        ele_num=np.zeros(b * S * ns2, np.int64), proj_cnt=np.zeros(b * S * npj, np.int64),
+        counter=np.zeros(b * 6, np.int64), draws=np.zeros(b, np.int64),
+        next624=np.zeros(b * 624, np.uint32), energies=np.zeros(2 * b))
+    err = err_buf()
+    rc = lib().oracle_physcal_samples(
+        namelist.encode(), zqp.encode(), ctypes.c_longlong(seed), *(ptr(out[k]) for k in (
+            "ele_idx", "ele_cfg", "ele_num", "proj_cnt", "counter", "draws", "next624", "energies")),
+        err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return d, out
+
+
+def step1_operands(namelist, cg=1, store=0, seed=1):
+    d = model_dims(namelist)
+    size = 1 + d["npara"]
+    e, ho, oo, o = np.zeros(1), np.zeros(size), np.zeros(2 * size), np.zeros(size)
+    err = err_buf()
+    rc = lib().oracle_step1_operands(namelist.encode(), cg, store, ctypes.c_longlong(seed), ptr(e),
+                                     ptr(ho), ptr(oo), ptr(o), size, err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return dict(energy=e, ho=ho, oo=oo, o=o)
+
+
+def run_opt(namelist, out_dir, walkers=1, nsteps=0, seed=-1, initial_def=""):
+    err = err_buf()
+    rc = lib().oracle_run_opt(namelist.encode(), initial_def.encode(), out_dir.encode(), walkers,
+                              nsteps, ctypes.c_longlong(seed), err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+
+
+def cg_fixed(mean, diag, samples, g, inv_w, shift, tol, max_iter, diag_scale=False, want_apply=False):
+    n = len(mean)
+    ns = samples.size // n
+    x = np.zeros(n)
+    z = np.zeros(n) if want_apply else None
+    st = lib().oracle_cg_fixed(n, ns, ptr(np.ascontiguousarray(mean)), ptr(np.ascontiguousarray(diag)),
+                               ptr(np.ascontiguousarray(samples)), ptr(np.ascontiguousarray(g)),
+                               ctypes.c_double(inv_w), ctypes.c_double(shift), ctypes.c_double(tol),
+                               max_iter, int(diag_scale), ptr(x), ptr(z) if z is not None else None)
+    return st, x, z
+
+
+def hexline(line):
+    import struct
+    return np.array([struct.unpack(">d", bytes.fromhex(v))[0] for v in line.split()])

@@ -1,0 +1,136 @@
+"""Pins the oracle (the CPU checker) to the reference's own golden vectors.
+
+Every fixture under tests/golden/ is output of the native C mVMC 1.4.0 program or of
+the C SFMT library, copied from the reference by tests/golden/make_golden.py.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+G = ol.GOLDEN
+
+
+def test_sfmt_first_words_match_c_library():
+    gold = json.load(open(os.path.join(G, "sfmt_first8.json")))
+    assert len(gold) == 6
+    for seed, words in gold.items():
+        assert ol.sfmt_words(int(seed), 8) == words, seed
+
+
+def read_pfapack(path):
+    vals = [float(l) for l in open(path) if l.strip() and not l.startswith("#") and " " not in l.strip()]
+    n = int(round(len(vals) ** 0.5))
+    return np.array(vals).reshape(n, n), n
+
+
+@pytest.mark.parametrize("name", sorted(os.listdir(os.path.join(G, "pfapack"))))
+def test_pfaffian_identities_on_reference_matrices(name):
+    # crates/pfapack/tests/fixed_matrix_identities.rs: Pf^2 = det, inverse residual <= 64 eps.
+    x, n = read_pfapack(os.path.join(G, "pfapack", name))
+    assert np.allclose(x, -x.T)
+    pf, inv, st = ol.pfinv_batch(x.T.ravel(), n, 1)
+    assert st[0] == 0
+    xi = inv.reshape(n, n).T
+    sign, logdet = np.linalg.slogdet(x)
+    assert sign > 0
+    assert abs(2 * np.log(abs(pf[0])) - logdet) <= n * 1e-13
+    eps = np.finfo(float).eps
+    resid = np.abs(xi @ x - np.eye(n)).max() / (np.abs(x).max() * np.abs(xi).max())
+    assert resid <= 64 * eps * n
+
+
+def test_pfaffian_zero_pivot_reports_row():
+    x = np.zeros((4, 4))
+    x[0, 1], x[1, 0] = 1.0, -1.0  # rank 2: the elimination meets a zero column
+    pf, inv, st = ol.pfinv_batch(x.T.ravel(), 4, 1)
+    assert st[0] > 0
+
+
+def read_state(path):
+    out = {}
+    for line in open(path):
+        p = line.split()
+        out[p[0]] = p[1:]
+    return out
+
+
+def test_sampler_reproduces_native_c_trajectory():
+    """Every saved configuration, projection counter, C Counter[0..6], draw count and
+    the next 624 SFMT words of two sample blocks of the native C sampler."""
+    d = os.path.join(G, "physcal_hubbard_chain_real")
+    dims, out = ol.physcal_samples(os.path.join(d, "inputs", "namelist.def"),
+                                   os.path.join(d, "zqp_opt.dat"), seed=1)
+    n, ns2, npj, S = 2 * dims["ne"], 2 * dims["nsite"], dims["nproj"], dims["nvmc_sample"]
+    for b in range(dims["data_qty_smp"]):
+        ref = read_state(os.path.join(d, "native-state", f"state_dump_{b:03d}.txt"))
+        for key, name, width in [("ele_idx", "ele_idx", n), ("ele_cfg", "ele_cfg", ns2),
+                                 ("ele_num", "ele_num", ns2), ("proj_cnt", "ele_proj_cnt", npj)]:
+            got = out[key][b * S * width:(b + 1) * S * width]
+            assert got.tolist() == [int(v) for v in ref[name]], (b, key)
+        assert out["counter"][b * 6:(b + 1) * 6].tolist() == [int(v) for v in ref["counter"][:6]]
+        assert int(out["draws"][b]) == int(ref["draws"][0])
+        assert out["next624"][b * 624:(b + 1) * 624].tolist() == [int(v) for v in ref["next624"]]
+
+
+def test_physcal_energy_matches_native_c_zvo_out():
+    d = os.path.join(G, "physcal_hubbard_chain_real")
+    dims, out = ol.physcal_samples(os.path.join(d, "inputs", "namelist.def"),
+                                   os.path.join(d, "zqp_opt.dat"), seed=1)
+    for b, idx in enumerate((7, 8)):
+        row = open(os.path.join(d, "expected", f"zvo_out_{idx:03d}.dat")).read().split()
+        etot, etot2 = float(row[0]), float(row[2])
+        assert abs(out["energies"][2 * b] - etot) <= 1e-12 * abs(etot)
+        assert abs(out["energies"][2 * b + 1] - etot2) <= 1e-12 * abs(etot2)
+
+
+def test_step1_sr_operands_match_native_c():
+    """crates/mvmc-core/tests/c_sr_operands_358.rs: ABS 1e-14 / REL 1e-13, energy 1e-12."""
+    d = os.path.join(G, "sr_operands_hubbard")
+    got = ol.step1_operands(os.path.join(d, "inputs", "namelist.def"), cg=1, store=0, seed=1)
+    ref = {}
+    for line in open(os.path.join(d, "hubbard-cg-store0.txt")):
+        if line.startswith("#"):
+            continue
+        name, rest = line.split(None, 1)
+        ref[name] = ol.hexline(rest)
+    assert abs(got["energy"][0] - ref["energy"][0]) <= 1e-12 * (1 + abs(ref["energy"][0]))
+    for name in ("ho", "oo", "o"):
+        r = ref[name]
+        a = got[name][: len(r)]
+        assert np.all(np.abs(a - r) <= 1e-14 + 1e-13 * np.abs(r)), name
+
+
+def read_cg_fixture(path):
+    lines = [l.rstrip("\n") for l in open(path) if not l.startswith("#")]
+    n, samples, cplx = (int(v) for v in lines[0].split())
+    assert cplx == 0
+    mean, diag, real = ol.hexline(lines[1]), ol.hexline(lines[2]), ol.hexline(lines[3])
+    g, expected_apply = ol.hexline(lines[5]), ol.hexline(lines[6])
+    limits = []
+    k = 7
+    while k + 2 < len(lines) + 1 and k < len(lines):
+        head = lines[k].split(" ", 2)
+        limits.append((int(head[0]), int(head[1]), ol.hexline(head[2])))
+        k += 3
+    return n, samples, mean, diag, real, g, expected_apply, limits
+
+
+@pytest.mark.parametrize("name,diag_scale", [("real.txt", False), ("real_diag_scale.txt", True)])
+def test_cg_recurrence_matches_native_c(name, diag_scale):
+    """C StochasticOptCG on fixed operands (tol 0, shift 1e-5): statuses exact,
+    S·g within the two-GEMV rounding budget, iterates within 1e-8 relative for the
+    first limits (CG amplifies roundoff after the residual drops)."""
+    n, samples, mean, diag, real, g, expected_apply, limits = read_cg_fixture(
+        os.path.join(G, "sr_cg", name))
+    _, _, z = ol.cg_fixed(mean, diag, real, g, 1.0 / samples, 1e-5, 0.0, 1, diag_scale, True)
+    budget = 8.0 * (n + samples) * np.finfo(float).eps
+    assert np.all(np.abs(z - expected_apply) <= budget + budget * np.abs(expected_apply))
+    for limit, status, x_ref in limits:
+        st, x, _ = ol.cg_fixed(mean, diag, real, g, 1.0 / samples, 1e-5, 0.0, limit, diag_scale)
+        assert st == status, limit
+        if limit <= 5:
+            assert np.allclose(x, x_ref, rtol=1e-8, atol=1e-12 * np.abs(x_ref).max()), limit

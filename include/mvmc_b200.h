@@ -1,0 +1,141 @@
+/* mvmc_b200.h — C ABI of the B200-native VMC sampling + SR hot path.
+ *
+ * The entry points replace the in-process stage seams of AtelierArith/mvmc-rs that the
+ * `mvmc` optimizer loop (crates/mvmc-core/src/run.rs:1226-1502, vmc_para_opt_timed)
+ * calls; each declaration names the reference interface it stands in for.
+ *
+ * Conventions: plain pointers and sizes; `int` status 0 = ok, > 0 = numeric status
+ * (1-based zero-pivot row), < 0 = error class (MVMC_B200_E*). No exceptions cross the
+ * ABI. A context owns one CUDA stream and its device buffers; it is thread-compatible,
+ * not thread-safe (stages are Send, not Sync: crates/mvmc-core/src/stage_backend.rs:1004).
+ * There is no CPU fallback: without a CUDA device every compute entry point returns
+ * MVMC_B200_ECUDA.
+ */
+#ifndef MVMC_B200_H
+#define MVMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MVMC_B200_OK 0
+#define MVMC_B200_EARG (-1)
+#define MVMC_B200_ECUDA (-2)
+#define MVMC_B200_EMODEL (-3)
+#define MVMC_B200_ENUMERIC (-4)
+#define MVMC_B200_ETIMEOUT (-5)
+#define MVMC_B200_ESTATE (-6)
+
+/* ---------------------------------------------------------------------------------
+ * Batched Pfaffian + inverse.
+ * Replaces PfaffianStages::pfaffian_inverse_batch(x, n, planes) -> PfInvBatch
+ * (crates/mvmc-core/src/stage_backend.rs:121-165): planes are column-major n×n back to
+ * back; `inv` receives the true X⁻¹ (the caller negates for InvM); `status[p]` is 0,
+ * the 1-based row of a zero pivot (PlaneOutcome::ZeroPivot), or -1 (NonFinite).
+ * Host buffers; the call allocates device memory.
+ * ------------------------------------------------------------------------------- */
+int mvmc_b200_pfinv_batch(const double* x, int n, int planes, double* pf, double* inv,
+                          int* status);
+
+/* Mixed sizes in one launch: plane p has side sizes[p] and starts where plane p-1 ends.
+ * precision 64 (FP64 sweep) or 32 (FP32 sweep, FP64 in/out). Host buffers. */
+int mvmc_b200_pfinv_batch_mixed(const double* x, const int* sizes, int planes, int precision,
+                                double* pf, double* inv, int* status);
+
+/* Device-buffer form (no allocation): sizes/offsets may be NULL for a uniform batch of
+ * side n_uniform; n_max bounds every side. stream is a cudaStream_t (NULL = default). */
+int mvmc_b200_pfinv_batch_device(const double* x, const int* sizes, const long long* offsets,
+                                 int n_uniform, int planes, int n_max, double* pf, double* inv,
+                                 int* status, int precision, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * Walker ensemble engine.
+ * ------------------------------------------------------------------------------- */
+typedef struct mvmc_b200_ctx mvmc_b200_ctx;
+
+typedef struct mvmc_b200_options {
+  int walkers;          /* W independent chains, walker w seeded RndSeed + w (multichain.rs:88) */
+  int precision;        /* 64: plain FP64 path; 32: FP32 rank-2 updates + FP64 refresh */
+  int refresh_sweeps;   /* FP32 path: FP64 refresh every this many sweeps (0 = C rule only) */
+  int saved_per_walker; /* samples saved per walker and SR step; 0 = NVMCSample (C semantics) */
+  long long seed;       /* < 0: RndSeed of modpara.def */
+  int device;           /* CUDA device ordinal */
+} mvmc_b200_options;
+
+void mvmc_b200_default_options(mvmc_b200_options* opt);
+
+/* Parse the Expert-mode namelist (crates/mvmc-expert-parsers, parse_expert_mode_files) and
+ * upload the model: Slater index tables, QP weights, projection index tables and the
+ * Transfer / CoulombIntra / CoulombInter / Hund term lists. Parameters are initialised as
+ * run_para_opt_timed does (run.rs:1696-1737: init_parameter per walker stream, optional
+ * initial.def, sync_modified). */
+int mvmc_b200_create(const char* namelist, const char* initial_def, const mvmc_b200_options* opt,
+                     mvmc_b200_ctx** out);
+void mvmc_b200_destroy(mvmc_b200_ctx* ctx);
+
+/* Dimensions: [nsite, ne, nqp, nproj, npara, saved_per_walker, walkers, n_orb]. */
+int mvmc_b200_dims(const mvmc_b200_ctx* ctx, int* dims);
+
+/* Current parameters (G, J, Slater order) as pack_variational_parameters (sync.rs:20). */
+int mvmc_b200_get_parameters(const mvmc_b200_ctx* ctx, double* params, int npara);
+int mvmc_b200_set_parameters(mvmc_b200_ctx* ctx, const double* params, int npara);
+
+/* One SR step's sampling for every walker: update_slater_elm (slater_update.rs:17) on the
+ * device, then vmc_make_sample_real_engine (sampling/driver.rs:175-438) with
+ * HostEngine::run_block's proposal loop (sampling/engine.rs:188-476) run resident on the
+ * device: SFMT19937 per walker, hop/exchange proposals, rank-2 updates, refresh when the
+ * accept window exceeds Nsite. Saved configurations stay on the device. */
+int mvmc_b200_sample(mvmc_b200_ctx* ctx);
+
+/* Download the saved configurations of the last mvmc_b200_sample (parity checks):
+ * ele_idx[W*S*nsize], ele_cfg[W*S*2Ns], ele_num[W*S*2Ns], proj_cnt[W*S*nproj],
+ * counters[W*6] (C Counter[0..6]), draws[W] (SFMT words consumed). Any pointer may be NULL. */
+int mvmc_b200_get_samples(const mvmc_b200_ctx* ctx, int64_t* ele_idx, int64_t* ele_cfg,
+                          int64_t* ele_num, int64_t* proj_cnt, int64_t* counters, int64_t* draws);
+
+/* Local measurement of every saved sample (MeasurementStages::measure_sample,
+ * stage_backend.rs:387-440; accumulate_observables_local, run.rs:2937-3614): Pfaffian and
+ * inverse, IP, local energy, O = [1, projection counts, ∂lnΨ/∂f] written as rows of the SR
+ * sample matrix (calculate_oo_store_real, observables.rs:297), then the rank-ordered
+ * reduction and weight average (average.rs:18-80). energy[5] = {Wc, <E>, <E²>, <Sz>, <Sz²>};
+ * ho[sr_size], oo[2*sr_size] (mean then diagonal) may be NULL. */
+int mvmc_b200_measure(mvmc_b200_ctx* ctx, double* energy, double* ho, double* oo);
+
+/* Rows of the SR sample matrix (W*S rows × sr_size, row-major) for parity checks. */
+int mvmc_b200_get_o_store(const mvmc_b200_ctx* ctx, double* o_store, long long count);
+/* Per-sample local energies (W*S). */
+int mvmc_b200_get_local_energies(const mvmc_b200_ctx* ctx, double* e_loc, long long count);
+
+/* SR-CG step: stochastic_opt_cg_with_reducer (sr_cg.rs:201-490) with
+ * SampledSrOperator::solve_with_product (sr_cg.rs:700-880) run on the device; S·v is
+ * Oᵀ(O·v)/W − ⟨O⟩(⟨O⟩·v) + δ·diag(S)·v. Updates the parameters (update_parameter_value,
+ * sr.rs:439) and applies sync_modified_parameter_local (sync.rs:87). sr_info receives
+ * {npara, nsmat, opt_cut, diag_cut, sdiag_max, sdiag_min, rmax, imax, info}; returns 0, or
+ * 1 when the update was non-finite and skipped, or < 0 on error. */
+int mvmc_b200_sr_cg(mvmc_b200_ctx* ctx, double* sr_info);
+
+/* Sticky device status word (first failing stage wins): MVMC_B200_DEV_* bits. */
+#define MVMC_B200_DEV_SINGULAR 1u
+#define MVMC_B200_DEV_NONFINITE 2u
+#define MVMC_B200_DEV_INITLOOPS 4u
+#define MVMC_B200_DEV_BOUNDS 8u
+#define MVMC_B200_DEV_CANDIDATE 16u
+int mvmc_b200_status(mvmc_b200_ctx* ctx, unsigned* device_status);
+
+/* The whole optimisation (run_para_opt_from_namelist, run.rs:1558; the `mvmc namelist.def`
+ * CLI path): NSROptItrStep steps of sample → measure → SR-CG → sync, writing zvo_out.dat,
+ * zvo_var.dat, zvo_SRinfo.dat and zqp_*opt.dat into out_dir. nsteps <= 0 keeps the
+ * modpara value. */
+int mvmc_b200_run_opt(const char* namelist, const char* initial_def, const char* out_dir,
+                      const mvmc_b200_options* opt, int nsteps);
+
+/* Last error message of the calling thread (empty when none). */
+const char* mvmc_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MVMC_B200_H */

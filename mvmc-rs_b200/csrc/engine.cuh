@@ -1,0 +1,64 @@
+// Device-side model and walker-ensemble state shared by the sampler, measurement and
+// SR kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace mvmcb {
+
+// Read-only model tables (device pointers) and dimensions.
+struct DevModel {
+  int ns, ne, n, ns2, nqp, nproj, n_gutz, n_jast, norb, nleg, nmp, nex_path;
+  int nterm, nintra, ninter, nhund;
+  int warmup, interval, saved;  // NVMCWarmUp, NVMCInterval, samples saved per walker
+  int sr_size;
+  const double* slater;    // [nqp][ns2][ns2] row-major
+  const float* slater32;   // FP32 copy (mixed path)
+  const double* qpw;       // [nqp] QPFullWeight (real)
+  const double* proj;      // [nproj] G then J parameter values
+  const int* gutz_idx;     // [ns]
+  const int* jast_idx;     // [ns*ns] (-1 undefined)
+  const double* gutz_site; // [ns] direct projection tables (observables.rs:1553)
+  const double* jast_pair; // [ns*ns]
+  const int* orb_idx;      // [ns*ns]
+  const int* orb_sgn;      // [ns*ns]
+  const int* trans;        // [nmp*ns] translated site
+  const int* trans_sgn;    // [nmp*ns] boundary sign (already 1 when periodic)
+  const double* spgl;      // [3*nleg]: cs, cc, ss
+  const int* tterm;        // [nterm*4]: i, si, j, sj
+  const double* tval;      // [nterm]
+  const int* intra_i;      // [nintra]
+  const double* intra_v;
+  const int* inter_ij;     // [ninter*2]
+  const double* inter_v;
+  const int* hund_ij;      // [nhund*2]
+  const double* hund_v;
+};
+
+// Per-walker persistent state, arrays of W entries each.
+struct DevWalkers {
+  int W;
+  uint32_t* sfmt;             // [W*624]
+  int* sfmt_idx;              // [W]
+  unsigned long long* draws;  // [W]
+  int* ele_idx;               // [W*n]
+  int* ele_cfg;               // [W*ns2]
+  int* ele_num;               // [W*ns2]
+  int* proj_cnt;              // [W*nproj]
+  int* burn;                  // [W]
+  void* inv;                  // [W*nqp*n*n] planes when not shared-memory resident
+  double* ws64;               // [W*n*n] FP64 refresh workspace (mixed path)
+  double* pf;                 // [W*nqp]
+  long long* counter;         // [W*6]
+  int* s_idx;                 // [W*saved*n]
+  int* s_cfg;                 // [W*saved*ns2]
+  int* s_num;                 // [W*saved*ns2]
+  int* s_cnt;                 // [W*saved*nproj]
+  unsigned* status;           // [1] sticky
+  int refresh_sweeps;         // mixed path: extra FP64 refresh cadence in sweeps (0 = off)
+};
+
+}  // namespace mvmcb

@@ -1,0 +1,147 @@
+// Skew-symmetric Gauss–Jordan sweep with 2×2 pivots: Pfaffian and inverse in one pass.
+//
+// For a skew matrix X (n even) the in-place Gauss–Jordan sweep over the index pair
+// (p, q) with pivot block [[0, a], [-a, 0]], a = X[p][q], keeps the matrix skew:
+//   A[i][j] += (rowq[i]·rowp[j] − rowp[i]·rowq[j]) / a        (i, j ∉ {p, q})
+//   A[p][j]  = rowq[j] / a,  A[q][j] = −rowp[j] / a,  A[p][q] = −1/a
+// where rowp, rowq are rows p and q before the sweep. After n/2 sweeps covering every
+// index once, A = X⁻¹ and Pf(X) = sgn(σ) Π a_k with σ = (p1 q1 p2 q2 …).
+// Pivoting: p = smallest unswept index, q = argmax_{unswept j≠p} |A[p][j]| (first
+// maximum) — the Parlett–Reid partial pivoting rule applied row-wise.
+//
+// This replaces pfapack's dsktf2 → utu2pfa → utu2inv pipeline
+// (crates/pfapack/src/ltl.rs:34-188, utu2.rs:52-110,338-515 of AtelierArith/mvmc-rs)
+// with one sweep of n/2 rank-2 updates: 2n³ flops on the full matrix (n³ on half),
+// no triangular solves, no permutation passes, every update a uniform data-parallel
+// rank-2 step.
+#pragma once
+
+#include "common.cuh"
+
+namespace mvmcb {
+
+template <typename T>
+struct GJShared {
+  T* rowp;      // [n] snapshot of row p
+  T* rowq;      // [n] snapshot of row q
+  int* swept;   // [n]
+  int* ctl;     // [4]: p, q, status, parity
+  double* pfv;  // [1] running product of pivots
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t gj_shared_bytes(int n) {
+  return 2 * sizeof(T) * static_cast<size_t>(n) + sizeof(int) * static_cast<size_t>(n) +
+         4 * sizeof(int) + sizeof(double) + 64;
+}
+
+template <typename T>
+__device__ __forceinline__ GJShared<T> gj_carve(unsigned char* base, int n) {
+  GJShared<T> s;
+  size_t off = 0;
+  s.pfv = reinterpret_cast<double*>(base + off);
+  off += 16;
+  s.rowp = reinterpret_cast<T*>(base + off);
+  off += sizeof(T) * n;
+  s.rowq = reinterpret_cast<T*>(base + off);
+  off += sizeof(T) * n;
+  off = (off + 15) & ~size_t(15);
+  s.swept = reinterpret_cast<int*>(base + off);
+  off += sizeof(int) * n;
+  s.ctl = reinterpret_cast<int*>(base + off);
+  return s;
+}
+
+// CTA-wide. A is row-major with leading dimension lda (shared or global memory).
+// On exit A holds X⁻¹; pf_out/status_out are valid in every thread.
+// status: 0 ok, k > 0 singular (1-based row of the zero pivot row), -1 non-finite Pf.
+template <typename T>
+__device__ void gj_pfinv(T* A, int lda, int n, const GJShared<T>& s, double& pf_out,
+                         int& status_out) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  for (int j = tid; j < n; j += nt) s.swept[j] = 0;
+  if (tid == 0) {
+    s.ctl[0] = 0;
+    s.ctl[2] = 0;
+    s.ctl[3] = 0;
+    *s.pfv = 1.0;
+  }
+  __syncthreads();
+  for (int k = 0; k < n / 2; ++k) {
+    const int p = s.ctl[0];
+    for (int j = tid; j < n; j += nt) s.rowp[j] = A[p * lda + j];
+    __syncthreads();
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = n;
+      for (int j = lane; j < n; j += 32) {
+        if (!s.swept[j] && j != p) {
+          const double v = fabs(static_cast<double>(s.rowp[j]));
+          if (v > best) {
+            best = v;
+            bi = j;
+          }
+        }
+      }
+      warp_argmax_first(best, bi);
+      const int q = __shfl_sync(0xffffffffu, bi, 0);
+      best = __shfl_sync(0xffffffffu, best, 0);
+      int cnt = 0;
+      for (int j = lane; j < n; j += 32) cnt += (!s.swept[j] && j > p && j < q) ? 1 : 0;
+      for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+      __syncwarp();
+      if (lane == 0) {
+        if (!(best > 0.0)) {
+          s.ctl[2] = p + 1;
+        } else {
+          *s.pfv *= static_cast<double>(s.rowp[q]);
+          s.ctl[3] += cnt;
+          s.ctl[1] = q;
+          s.swept[p] = 1;
+          s.swept[q] = 1;
+        }
+      }
+      __syncwarp();
+      int nxt = n;
+      for (int j = lane; j < n; j += 32)
+        if (!s.swept[j] && j < nxt) nxt = j;
+      for (int off = 16; off > 0; off >>= 1) nxt = min(nxt, __shfl_xor_sync(0xffffffffu, nxt, off));
+      if (lane == 0) s.ctl[0] = nxt < n ? nxt : 0;
+    }
+    __syncthreads();
+    if (s.ctl[2] != 0) break;
+    const int q = s.ctl[1];
+    for (int j = tid; j < n; j += nt) s.rowq[j] = A[q * lda + j];
+    __syncthreads();
+    const T ia = T(1) / s.rowp[q];
+    for (int i = warp; i < n; i += nwarp) {
+      const T rpi = s.rowp[i], rqi = s.rowq[i];
+      T* Ai = A + i * lda;
+      if (i == p) {
+        for (int j = lane; j < n; j += 32) Ai[j] = (j == q) ? -ia : (j == p ? T(0) : s.rowq[j] * ia);
+      } else if (i == q) {
+        for (int j = lane; j < n; j += 32) Ai[j] = (j == p) ? ia : (j == q ? T(0) : -s.rowp[j] * ia);
+      } else {
+        for (int j = lane; j < n; j += 32) {
+          T v;
+          if (j == p) v = -rqi * ia;
+          else if (j == q) v = rpi * ia;
+          else v = Ai[j] + (rqi * s.rowp[j] - rpi * s.rowq[j]) * ia;
+          Ai[j] = v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int status = s.ctl[2];
+  double pf = (s.ctl[3] & 1) ? -*s.pfv : *s.pfv;
+  int st = status;
+  if (st == 0 && !isfinite(pf)) st = -1;
+  if (st != 0) pf = 0.0;
+  pf_out = pf;
+  status_out = st;
+  __syncthreads();
+}
+
+}  // namespace mvmcb

@@ -1,0 +1,168 @@
+"""Python binding of the mvmc-b200 C ABI (include/mvmc_b200.h) through ctypes.
+
+The library is built in-tree (`make -C mvmc-rs_b200`, or `__graft_entry__.build()`).
+There is no CPU fallback: loading fails loudly when the shared library is missing, and
+every compute call raises when the CUDA path reports an error.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libmvmc_b200.so")
+_LIB = None
+
+EXPORTS = [
+    "mvmc_b200_pfinv_batch", "mvmc_b200_pfinv_batch_mixed", "mvmc_b200_pfinv_batch_device",
+    "mvmc_b200_default_options", "mvmc_b200_create", "mvmc_b200_destroy", "mvmc_b200_dims",
+    "mvmc_b200_get_parameters", "mvmc_b200_set_parameters", "mvmc_b200_sample",
+    "mvmc_b200_get_samples", "mvmc_b200_measure", "mvmc_b200_get_o_store",
+    "mvmc_b200_get_local_energies", "mvmc_b200_sr_cg", "mvmc_b200_status", "mvmc_b200_run_opt",
+    "mvmc_b200_last_error",
+]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("walkers", ctypes.c_int), ("precision", ctypes.c_int),
+                ("refresh_sweeps", ctypes.c_int), ("saved_per_walker", ctypes.c_int),
+                ("seed", ctypes.c_longlong), ("device", ctypes.c_int)]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"mvmc_b200: CUDA library not built ({LIB_PATH}); run make -C mvmc-rs_b200")
+        _LIB = ctypes.CDLL(LIB_PATH)
+        _LIB.mvmc_b200_last_error.restype = ctypes.c_char_p
+    return _LIB
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _check(rc, what):
+    if rc < 0:
+        msg = lib().mvmc_b200_last_error()
+        raise RuntimeError(f"{what} failed with status {rc}: {msg.decode() if msg else ''}")
+    return rc
+
+
+def pfinv_batch(x_colmajor, n, planes):
+    """Batched Pfaffian and inverse of column-major skew planes (true X^-1 returned)."""
+    x = np.ascontiguousarray(x_colmajor, dtype=np.float64)
+    pf = np.zeros(planes)
+    inv = np.zeros(planes * n * n)
+    st = np.zeros(planes, dtype=np.int32)
+    _check(lib().mvmc_b200_pfinv_batch(_ptr(x), n, planes, _ptr(pf), _ptr(inv), _ptr(st)), "pfinv_batch")
+    return pf, inv, st
+
+
+def pfinv_batch_mixed(x, sizes, precision=64):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+    planes = len(sizes)
+    pf = np.zeros(planes)
+    inv = np.zeros(x.size)
+    st = np.zeros(planes, dtype=np.int32)
+    _check(lib().mvmc_b200_pfinv_batch_mixed(_ptr(x), _ptr(sizes), planes, precision, _ptr(pf),
+                                             _ptr(inv), _ptr(st)), "pfinv_batch_mixed")
+    return pf, inv, st
+
+
+def default_options(**kw):
+    o = Options()
+    lib().mvmc_b200_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Engine:
+    """Walker-ensemble engine: sample → measure → SR-CG on the device."""
+
+    def __init__(self, namelist, initial_def="", **options):
+        self.opt = default_options(**options)
+        self.ctx = ctypes.c_void_p()
+        _check(lib().mvmc_b200_create(namelist.encode(), (initial_def or "").encode(),
+                                      ctypes.byref(self.opt), ctypes.byref(self.ctx)), "create")
+        d = (ctypes.c_int * 8)()
+        _check(lib().mvmc_b200_dims(self.ctx, d), "dims")
+        keys = ["nsite", "ne", "nqp", "nproj", "npara", "saved", "walkers", "n_orb"]
+        self.dims = dict(zip(keys, list(d)))
+
+    def close(self):
+        if self.ctx:
+            lib().mvmc_b200_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def sr_size(self):
+        return 1 + self.dims["npara"]
+
+    def parameters(self):
+        p = np.zeros(self.dims["npara"])
+        _check(lib().mvmc_b200_get_parameters(self.ctx, _ptr(p), len(p)), "get_parameters")
+        return p
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        _check(lib().mvmc_b200_set_parameters(self.ctx, _ptr(p), len(p)), "set_parameters")
+
+    def sample(self):
+        _check(lib().mvmc_b200_sample(self.ctx), "sample")
+
+    def samples(self):
+        d = self.dims
+        W, S, n, ns2 = d["walkers"], d["saved"], 2 * d["ne"], 2 * d["nsite"]
+        out = dict(ele_idx=np.zeros(W * S * n, np.int64), ele_cfg=np.zeros(W * S * ns2, np.int64),
+                   ele_num=np.zeros(W * S * ns2, np.int64),
+                   proj_cnt=np.zeros(W * S * d["nproj"], np.int64),
+                   counter=np.zeros(W * 6, np.int64), draws=np.zeros(W, np.int64))
+        _check(lib().mvmc_b200_get_samples(self.ctx, *(_ptr(out[k]) for k in (
+            "ele_idx", "ele_cfg", "ele_num", "proj_cnt", "counter", "draws"))), "get_samples")
+        return out
+
+    def measure(self):
+        e = np.zeros(5)
+        ho = np.zeros(self.sr_size)
+        oo = np.zeros(2 * self.sr_size)
+        _check(lib().mvmc_b200_measure(self.ctx, _ptr(e), _ptr(ho), _ptr(oo)), "measure")
+        return e, ho, oo
+
+    def o_store(self):
+        d = self.dims
+        out = np.zeros(d["walkers"] * d["saved"] * self.sr_size)
+        _check(lib().mvmc_b200_get_o_store(self.ctx, _ptr(out), ctypes.c_longlong(out.size)), "o_store")
+        return out.reshape(d["walkers"] * d["saved"], self.sr_size)
+
+    def local_energies(self):
+        d = self.dims
+        out = np.zeros(d["walkers"] * d["saved"])
+        _check(lib().mvmc_b200_get_local_energies(self.ctx, _ptr(out), ctypes.c_longlong(out.size)),
+               "local_energies")
+        return out
+
+    def sr_cg(self):
+        info = np.zeros(9)
+        rc = _check(lib().mvmc_b200_sr_cg(self.ctx, _ptr(info)), "sr_cg")
+        return rc, info
+
+    def status(self):
+        s = ctypes.c_uint()
+        _check(lib().mvmc_b200_status(self.ctx, ctypes.byref(s)), "status")
+        return s.value
+
+
+def run_opt(namelist, out_dir, initial_def="", nsteps=0, **options):
+    opt = default_options(**options)
+    _check(lib().mvmc_b200_run_opt(namelist.encode(), (initial_def or "").encode(), out_dir.encode(),
+                                   ctypes.byref(opt), nsteps), "run_opt")

@@ -116,6 +116,13 @@ int mvmc_b200_get_local_energies(const mvmc_b200_ctx* ctx, double* e_loc, long l
  * 1 when the update was non-finite and skipped, or < 0 on error. */
 int mvmc_b200_sr_cg(mvmc_b200_ctx* ctx, double* sr_info);
 
+/* SR-CG on fixed operands (SrStages::cg_step, crates/mvmc-core/src/sr_backend.rs:193-297;
+ * the recurrence of SampledSrOperator::solve_with_product, sr_cg.rs:700-880). samples is
+ * [ns][na] row-major; status receives the C status (iterations, or -(iter+1)). Host buffers. */
+int mvmc_b200_cg_solve(const double* samples, long long ns, int na, const double* mean,
+                       const double* diag, const double* g, double inv_w, double shift, double tol,
+                       int max_iter, int diag_scale, double* x, long long* status);
+
 /* Sticky device status word (first failing stage wins): MVMC_B200_DEV_* bits. */
 #define MVMC_B200_DEV_SINGULAR 1u
 #define MVMC_B200_DEV_NONFINITE 2u

@@ -1,0 +1,655 @@
+// Walker-ensemble engine behind the C ABI: model upload, the Slater table (K0), and the
+// sample → measure → SR-CG stages of one optimisation step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mvmc_b200.h"
+#include "../host/abi_common.h"
+#include "../host/expert.h"
+#include "common.cuh"
+#include "engine.cuh"
+#include "sfmt.cuh"
+
+namespace mvmcb {
+
+int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStream_t stream);
+bool sample_planes_in_smem(const DevModel& m, int precision, int limit);
+int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
+                   const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
+                   double* eloc, int* valid, unsigned* status, cudaStream_t stream);
+int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,
+                  const int* valid, const int* s_num, double* wsum, double* tot, cudaStream_t stream);
+int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
+                         double* oa, cudaStream_t stream);
+int launch_sr_cg(CgArgs a, cudaStream_t stream);
+int cg_grid_blocks();
+
+// K0: SlaterElm[q][rs_i][rs_j] from the Slater parameters (update_slater_elm,
+// crates/mvmc-core/src/slater_update.rs:17-120).
+__global__ void k_slater_table(int ns, int nqp, int nleg, int nmp, const double* __restrict__ f,
+                               const int* __restrict__ orb_idx, const int* __restrict__ orb_sgn,
+                               const int* __restrict__ trans, const int* __restrict__ trans_sgn,
+                               const double* __restrict__ spgl, double* __restrict__ out,
+                               float* __restrict__ out32) {
+  const int ns2 = 2 * ns;
+  const long long total = static_cast<long long>(nqp) * ns * ns;
+  for (long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; k < total;
+       k += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int qp = static_cast<int>(k / (static_cast<long long>(ns) * ns));
+    const int rem = static_cast<int>(k - static_cast<long long>(qp) * ns * ns);
+    const int ri = rem / ns, rj = rem - ri * ns;
+    const int mpidx = (qp % (nleg * nmp)) / nleg, spidx = qp % nleg;
+    const double cs = spgl[spidx], cc = spgl[nleg + spidx], ss = spgl[2 * nleg + spidx];
+    const int tri = trans[mpidx * ns + ri], trj = trans[mpidx * ns + rj];
+    const int qpsgn = trans_sgn[mpidx * ns + ri] * trans_sgn[mpidx * ns + rj];
+    const int iij = orb_idx[tri * ns + trj], iji = orb_idx[trj * ns + tri];
+    double* p = out + static_cast<size_t>(qp) * ns2 * ns2;
+    float* p32 = out32 + static_cast<size_t>(qp) * ns2 * ns2;
+    double v00 = 0, v01 = 0, v10 = 0, v11 = 0;
+    if (iij >= 0 && iji >= 0) {
+      const double sij = f[iij] * static_cast<double>(orb_sgn[tri * ns + trj] * qpsgn);
+      const double sji = f[iji] * static_cast<double>(orb_sgn[trj * ns + tri] * qpsgn);
+      v00 = -(sij - sji) * cs;
+      v01 = sij * cc + sji * ss;
+      v10 = -sij * ss - sji * cc;
+      v11 = (sij - sji) * cs;
+    }
+    p[ri * ns2 + rj] = v00;
+    p[ri * ns2 + rj + ns] = v01;
+    p[(ri + ns) * ns2 + rj] = v10;
+    p[(ri + ns) * ns2 + rj + ns] = v11;
+    p32[ri * ns2 + rj] = static_cast<float>(v00);
+    p32[ri * ns2 + rj + ns] = static_cast<float>(v01);
+    p32[(ri + ns) * ns2 + rj] = static_cast<float>(v10);
+    p32[(ri + ns) * ns2 + rj + ns] = static_cast<float>(v11);
+  }
+}
+
+}  // namespace mvmcb
+
+using namespace mvmcb;
+
+struct mvmc_b200_ctx {
+  mvmc::Model m;
+  mvmc_b200_options opt;
+  int W = 1, S = 1;
+  cudaStream_t stream = nullptr;
+  DevModel dm{};
+  DevWalkers dw{};
+  std::vector<void*> allocs;
+  double* d_f = nullptr;
+  double* d_proj = nullptr;
+  double* d_gsite = nullptr;
+  double* d_jpair = nullptr;
+  double* d_slater = nullptr;
+  float* d_slater32 = nullptr;
+  double* d_ostore = nullptr;
+  double* d_eloc = nullptr;
+  int* d_valid = nullptr;
+  double* d_wsum = nullptr;
+  double* d_tot = nullptr;
+  double* d_gws = nullptr;
+  int gws_blocks = 0;
+  // SR-CG buffers
+  double* d_oa = nullptr;
+  size_t oa_cap = 0;
+  double* d_cgvec = nullptr;  // mean, diag, g, x, r, d, q
+  size_t cgvec_cap = 0;
+  double* d_y = nullptr;
+  double* d_part = nullptr;
+  size_t part_cap = 0;
+  double* d_red = nullptr;
+  double* d_scal = nullptr;
+  int* d_map = nullptr;
+  size_t map_cap = 0;
+  std::vector<double> tot;  // host copy of the last reduction
+  bool sampled = false, measured = false;
+
+  template <typename T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    if (count == 0) count = 1;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess)
+      throw std::runtime_error("cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <typename T>
+  T* upload(const std::vector<T>& v) {
+    T* p = alloc<T>(v.size());
+    if (!v.empty() && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+      throw std::runtime_error("cudaMemcpy upload failed");
+    return p;
+  }
+  ~mvmc_b200_ctx() {
+    for (void* p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void upload_parameters(mvmc_b200_ctx* c) {
+  const mvmc::Model& m = c->m;
+  const int ns = m.nsite;
+  std::vector<double> proj = m.gutz;
+  proj.insert(proj.end(), m.jast.begin(), m.jast.end());
+  std::vector<double> gsite(ns, 0.0), jpair(static_cast<size_t>(ns) * ns, 0.0);
+  for (int r = 0; r < ns; ++r) {
+    const int g = m.gutz_idx[r];
+    if (m.n_gutz > 0 && g >= 0 && g < m.n_gutz) gsite[r] = m.gutz[g];
+  }
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < ns; ++b) {
+      if (a == b || m.n_jast == 0) continue;
+      const int j = m.jast_idx[std::min(a, b) * ns + std::max(a, b)];
+      if (j >= 0 && j < m.n_jast) jpair[static_cast<size_t>(a) * ns + b] = m.jast[j];
+    }
+  check(cudaMemcpyAsync(c->d_f, m.slater.data(), sizeof(double) * std::max<size_t>(1, m.slater.size()),
+                        cudaMemcpyHostToDevice, c->stream), "upload f");
+  if (!proj.empty())
+    check(cudaMemcpyAsync(c->d_proj, proj.data(), sizeof(double) * proj.size(), cudaMemcpyHostToDevice, c->stream),
+          "upload proj");
+  check(cudaMemcpyAsync(c->d_gsite, gsite.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c->stream), "upload gsite");
+  check(cudaMemcpyAsync(c->d_jpair, jpair.data(), sizeof(double) * jpair.size(), cudaMemcpyHostToDevice, c->stream),
+        "upload jpair");
+  const long long total = static_cast<long long>(m.nqp) * ns * ns;
+  const int grid = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
+  k_slater_table<<<std::max(1, grid), 256, 0, c->stream>>>(
+      ns, m.nqp, std::max(1, m.nsp_gauss_leg), m.mp_trans(), c->d_f, c->dm.orb_idx, c->dm.orb_sgn, c->dm.trans,
+      c->dm.trans_sgn, c->dm.spgl, c->d_slater, c->d_slater32);
+  check(cudaGetLastError(), "slater table kernel");
+  check(cudaStreamSynchronize(c->stream), "parameter upload");
+}
+
+void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_def, const mvmc_b200_options& opt) {
+  c->opt = opt;
+  check(cudaSetDevice(opt.device), "cudaSetDevice");
+  check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  mvmc::Model& m = c->m;
+  m = mvmc::read_expert(namelist);
+  if (m.nsrcg == 0) m.nsrcg = 1;  // the device path solves SR by CG
+  c->W = std::max(1, opt.walkers);
+  c->S = opt.saved_per_walker > 0 ? opt.saved_per_walker : m.nvmc_sample;
+  if (opt.precision != 64 && opt.precision != 32) throw std::runtime_error("precision must be 64 or 32");
+  // walker streams: seed RndSeed + w, each consuming init_parameter draws (multichain.rs:88)
+  const long long base = opt.seed >= 0 ? opt.seed : m.rnd_seed;
+  std::vector<uint32_t> sf(static_cast<size_t>(c->W) * kSfmtN32);
+  std::vector<int> sf_idx(c->W);
+  std::vector<unsigned long long> draws(c->W);
+  for (int w = 0; w < c->W; ++w) {
+    const long long s = base + w;
+    if (s < 0 || s > 0xffffffffLL) throw std::runtime_error("walker seed outside the UInt32 range");
+    uint32_t* st = sf.data() + static_cast<size_t>(w) * kSfmtN32;
+    sfmt_seed(st, &sf_idx[w], static_cast<uint32_t>(s));
+    SfmtRef rng{st, &sf_idx[w], &draws[w]};
+    mvmc::Model tmp = m;
+    mvmc::init_parameter(tmp, [&]() { return rng.real2(); });
+    if (w == 0) {
+      m.gutz = tmp.gutz;
+      m.jast = tmp.jast;
+      m.slater = tmp.slater;
+    }
+  }
+  if (initial_def && *initial_def) {
+    std::string why;
+    if (!mvmc::read_para_triples(m, initial_def, &why)) throw std::runtime_error(std::string("initial.def: ") + why);
+  }
+  mvmc::sync_modified_parameter(m, true);
+  mvmc::init_qp_weight(m);
+
+  const int ns = m.nsite, n = m.nsize(), ns2 = 2 * ns, nqp = m.nqp, nproj = m.nproj();
+  DevModel& dm = c->dm;
+  dm.ns = ns; dm.ne = m.ne; dm.n = n; dm.ns2 = ns2; dm.nqp = nqp; dm.nproj = nproj;
+  dm.n_gutz = m.n_gutz; dm.n_jast = m.n_jast; dm.norb = m.n_orb;
+  dm.nleg = std::max(1, m.nsp_gauss_leg); dm.nmp = m.mp_trans(); dm.nex_path = m.nex_update_path;
+  dm.warmup = m.nvmc_warmup; dm.interval = m.nvmc_interval; dm.saved = c->S;
+  dm.sr_size = m.sr_size();
+  // projection / orbital / translation tables
+  std::vector<int> trans(static_cast<size_t>(dm.nmp) * ns), trans_sgn(trans.size());
+  for (int mp = 0; mp < dm.nmp; ++mp)
+    for (int r = 0; r < ns; ++r) mvmc::translated_site(m, r, mp, &trans[mp * ns + r], &trans_sgn[mp * ns + r]);
+  std::vector<double> spgl;
+  spgl.insert(spgl.end(), m.spgl_cs.begin(), m.spgl_cs.end());
+  spgl.insert(spgl.end(), m.spgl_cc.begin(), m.spgl_cc.end());
+  spgl.insert(spgl.end(), m.spgl_ss.begin(), m.spgl_ss.end());
+  std::vector<int> tterm;
+  std::vector<double> tval;
+  for (const auto& t : m.transfer) {
+    if (t.i < 0 || t.j < 0 || t.i >= ns || t.j >= ns) continue;
+    tterm.insert(tterm.end(), {t.i, t.si, t.j, t.sj});
+    tval.push_back(t.t);
+  }
+  std::vector<int> intra_i, inter_ij, hund_ij;
+  std::vector<double> intra_v, inter_v, hund_v;
+  for (const auto& t : m.coulomb_intra) if (t.i >= 0 && t.i < ns) { intra_i.push_back(t.i); intra_v.push_back(t.v); }
+  for (const auto& t : m.coulomb_inter) if (t.i >= 0 && t.j >= 0 && t.i < ns && t.j < ns) { inter_ij.insert(inter_ij.end(), {t.i, t.j}); inter_v.push_back(t.v); }
+  for (const auto& t : m.hund) if (t.i >= 0 && t.j >= 0 && t.i < ns && t.j < ns) { hund_ij.insert(hund_ij.end(), {t.i, t.j}); hund_v.push_back(t.v); }
+  dm.nterm = static_cast<int>(tval.size());
+  dm.nintra = static_cast<int>(intra_v.size());
+  dm.ninter = static_cast<int>(inter_v.size());
+  dm.nhund = static_cast<int>(hund_v.size());
+  dm.qpw = c->upload(m.qp_weight);
+  dm.gutz_idx = c->upload(m.gutz_idx);
+  dm.jast_idx = c->upload(m.jast_idx);
+  dm.orb_idx = c->upload(m.orb_idx);
+  dm.orb_sgn = c->upload(m.orb_sgn);
+  dm.trans = c->upload(trans);
+  dm.trans_sgn = c->upload(trans_sgn);
+  dm.spgl = c->upload(spgl);
+  dm.tterm = c->upload(tterm);
+  dm.tval = c->upload(tval);
+  dm.intra_i = c->upload(intra_i);
+  dm.intra_v = c->upload(intra_v);
+  dm.inter_ij = c->upload(inter_ij);
+  dm.inter_v = c->upload(inter_v);
+  dm.hund_ij = c->upload(hund_ij);
+  dm.hund_v = c->upload(hund_v);
+  c->d_f = c->alloc<double>(m.n_orb);
+  c->d_proj = c->alloc<double>(nproj);
+  c->d_gsite = c->alloc<double>(ns);
+  c->d_jpair = c->alloc<double>(static_cast<size_t>(ns) * ns);
+  c->d_slater = c->alloc<double>(static_cast<size_t>(nqp) * ns2 * ns2);
+  c->d_slater32 = c->alloc<float>(static_cast<size_t>(nqp) * ns2 * ns2);
+  dm.slater = c->d_slater;
+  dm.slater32 = c->d_slater32;
+  dm.proj = c->d_proj;
+  dm.gutz_site = c->d_gsite;
+  dm.jast_pair = c->d_jpair;
+
+  // walkers
+  DevWalkers& dw = c->dw;
+  const int W = c->W, S = c->S;
+  dw.W = W;
+  dw.sfmt = c->upload(sf);
+  dw.sfmt_idx = c->upload(sf_idx);
+  dw.draws = c->upload(draws);
+  dw.ele_idx = c->alloc<int>(static_cast<size_t>(W) * n);
+  dw.ele_cfg = c->alloc<int>(static_cast<size_t>(W) * ns2);
+  dw.ele_num = c->alloc<int>(static_cast<size_t>(W) * ns2);
+  dw.proj_cnt = c->alloc<int>(static_cast<size_t>(W) * std::max(1, nproj));
+  dw.burn = c->alloc<int>(W);
+  check(cudaMemset(dw.burn, 0, sizeof(int) * W), "memset burn");
+  dw.pf = c->alloc<double>(static_cast<size_t>(W) * nqp);
+  dw.counter = c->alloc<long long>(static_cast<size_t>(W) * 6);
+  dw.s_idx = c->alloc<int>(static_cast<size_t>(W) * S * n);
+  dw.s_cfg = c->alloc<int>(static_cast<size_t>(W) * S * ns2);
+  dw.s_num = c->alloc<int>(static_cast<size_t>(W) * S * ns2);
+  dw.s_cnt = c->alloc<int>(static_cast<size_t>(W) * S * std::max(1, nproj));
+  dw.status = c->alloc<unsigned>(1);
+  check(cudaMemset(dw.status, 0, sizeof(unsigned)), "memset status");
+  dw.refresh_sweeps = opt.refresh_sweeps;
+  int dev = 0, limit = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t nn = static_cast<size_t>(n) * n;
+  const bool smem = sample_planes_in_smem(dm, opt.precision, limit);
+  dw.inv = nullptr;
+  dw.ws64 = nullptr;
+  if (!smem) {
+    if (opt.precision == 64) dw.inv = c->alloc<double>(static_cast<size_t>(W) * nqp * nn);
+    else dw.inv = c->alloc<float>(static_cast<size_t>(W) * nqp * nn);
+  }
+  if (opt.precision == 32) dw.ws64 = c->alloc<double>(static_cast<size_t>(W) * nn);
+  // measurement
+  const size_t rows = static_cast<size_t>(W) * S;
+  c->d_ostore = c->alloc<double>(rows * dm.sr_size);
+  c->d_eloc = c->alloc<double>(rows);
+  c->d_valid = c->alloc<int>(rows);
+  c->d_wsum = c->alloc<double>(static_cast<size_t>(W) * (5 + 3 * dm.sr_size));
+  c->d_tot = c->alloc<double>(5 + 3 * dm.sr_size);
+  c->gws_blocks = std::min<int>(static_cast<int>(rows), sms * 8);
+  c->d_gws = c->alloc<double>(static_cast<size_t>(c->gws_blocks) * nn);
+  c->d_red = c->alloc<double>(4096);
+  c->d_scal = c->alloc<double>(8);
+  upload_parameters(c);
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    mvmcb::set_last_error(e.what());
+    const std::string what = e.what();
+    if (what.find("cuda") != std::string::npos || what.find("CUDA") != std::string::npos) return MVMC_B200_ECUDA;
+    return MVMC_B200_EMODEL;
+  }
+}
+
+int do_measure(mvmc_b200_ctx* c) {
+  const int rows = c->W * c->S;
+  int rc = launch_measure(c->dm, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, rows, c->d_gws,
+                          c->gws_blocks, c->d_ostore, c->d_eloc, c->d_valid, c->dw.status, c->stream);
+  if (rc != kOk) return rc;
+  rc = launch_reduce(c->dm, c->W, c->S, c->d_ostore, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
+                     c->stream);
+  if (rc != kOk) return rc;
+  c->tot.assign(5 + 3 * c->dm.sr_size, 0.0);
+  check(cudaMemcpyAsync(c->tot.data(), c->d_tot, sizeof(double) * c->tot.size(), cudaMemcpyDeviceToHost, c->stream),
+        "download reduction");
+  check(cudaStreamSynchronize(c->stream), "measure");
+  c->measured = true;
+  return kOk;
+}
+
+// stochastic_opt_cg_with_reducer (sr_cg.rs:201-490) around the device solve.
+int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
+  mvmc::Model& m = c->m;
+  const int size = m.sr_size(), npara = m.npara();
+  if (!c->measured) return MVMC_B200_ESTATE;
+  if (m.rescale_smat) throw std::runtime_error("RescaleSmat is not supported by the device SR path");
+  const double wc = c->tot[0];
+  const double* ho = c->tot.data() + 5;
+  const double* mean_all = c->tot.data() + 5 + size;
+  const double* diag_all = c->tot.data() + 5 + 2 * size;
+  std::vector<double> var(npara);
+  for (int pi = 0; pi < npara; ++pi) var[pi] = diag_all[pi + 1] - mean_all[pi + 1] * mean_all[pi + 1];
+  double vmax = -INFINITY, vmin = INFINITY;
+  bool any_nan = false;
+  for (double v : var) {
+    if (std::isnan(v)) any_nan = true;
+    vmax = std::fmax(vmax, v);
+    vmin = std::fmin(vmin, v);
+  }
+  if (any_nan) vmax = vmin = NAN;
+  const double threshold = vmax * m.red_cut;
+  std::vector<int> map;
+  int opt_cut = 0, diag_cut = 0;
+  for (int pi = 0; pi < npara; ++pi) {
+    const bool optimised = static_cast<size_t>(2 * pi) < m.opt_flags.size() && m.opt_flags[2 * pi] == 1;
+    if (!optimised) ++opt_cut;
+    else if (var[pi] < threshold) ++diag_cut;
+    else map.push_back(pi);
+  }
+  if (info_out) std::fill(info_out, info_out + 9, 0.0);
+  if (map.empty()) return 0;
+  const int na = static_cast<int>(map.size());
+  std::vector<double> vecs(static_cast<size_t>(3) * na);
+  const double dt = 2.0 * m.step_dt;
+  for (int si = 0; si < na; ++si) {
+    const int idx = map[si] + 1;
+    vecs[si] = mean_all[idx];
+    vecs[na + si] = var[map[si]];
+    vecs[2 * na + si] = -dt * (ho[idx] - ho[0] * mean_all[idx]);
+  }
+  const long long ns = static_cast<long long>(c->W) * c->S;
+  if (static_cast<size_t>(ns) * na > c->oa_cap) {
+    c->d_oa = c->alloc<double>(static_cast<size_t>(ns) * na);
+    c->oa_cap = static_cast<size_t>(ns) * na;
+    c->d_y = c->alloc<double>(ns);
+  }
+  if (static_cast<size_t>(7) * na > c->cgvec_cap) {
+    c->d_cgvec = c->alloc<double>(static_cast<size_t>(7) * na);
+    c->cgvec_cap = static_cast<size_t>(7) * na;
+  }
+  if (static_cast<size_t>(na) > c->map_cap) {
+    c->d_map = c->alloc<int>(na);
+    c->map_cap = na;
+  }
+  const int blocks = cg_grid_blocks();
+  const int ntile = (na + 255) / 256;
+  const int nchunk = static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, blocks / ntile))));
+  if (static_cast<size_t>(nchunk) * na > c->part_cap) {
+    c->d_part = c->alloc<double>(static_cast<size_t>(nchunk) * na);
+    c->part_cap = static_cast<size_t>(nchunk) * na;
+  }
+  check(cudaMemcpyAsync(c->d_map, map.data(), sizeof(int) * na, cudaMemcpyHostToDevice, c->stream), "upload map");
+  check(cudaMemcpyAsync(c->d_cgvec, vecs.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, c->stream),
+        "upload cg vectors");
+  int rc = launch_gather_active(c->d_ostore, size, ns, c->d_map, na, c->d_oa, c->stream);
+  if (rc != kOk) return rc;
+  CgArgs a;
+  a.O = c->d_oa;
+  a.mean = c->d_cgvec;
+  a.diag = c->d_cgvec + na;
+  a.g = c->d_cgvec + 2 * na;
+  a.x = c->d_cgvec + 3 * na;
+  a.r = c->d_cgvec + 4 * na;
+  a.d = c->d_cgvec + 5 * na;
+  a.q = c->d_cgvec + 6 * na;
+  a.y = c->d_y;
+  a.part = c->d_part;
+  a.red = c->d_red;
+  a.scal = c->d_scal;
+  a.ns = ns;
+  a.na = na;
+  a.nchunk = nchunk;
+  a.max_iter = m.cg_max_iter > 0 ? m.cg_max_iter : na;
+  a.diag_scale = m.diag_scale ? 1 : 0;
+  a.inv_w = 1.0 / wc;
+  a.shift = m.sta_del;
+  a.tol = m.cg_tol;
+  rc = launch_sr_cg(a, c->stream);
+  if (rc != kOk) return rc;
+  std::vector<double> x(na), scal(8);
+  check(cudaMemcpyAsync(x.data(), a.x, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
+  check(cudaMemcpyAsync(scal.data(), c->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->stream), "download scal");
+  check(cudaStreamSynchronize(c->stream), "sr-cg");
+  long long status = static_cast<long long>(scal[1]);
+  long long info = status;
+  if (status < 0) {
+    const long long fallback_iter = std::max(-status - 1, 0LL);
+    if (m.cg_fallback) {
+      a.diag_scale = !a.diag_scale;
+      rc = launch_sr_cg(a, c->stream);
+      if (rc != kOk) return rc;
+      check(cudaMemcpyAsync(x.data(), a.x, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
+      check(cudaMemcpyAsync(scal.data(), c->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->stream), "download");
+      check(cudaStreamSynchronize(c->stream), "sr-cg fallback");
+      info = -(fallback_iter + 1);
+      if (static_cast<long long>(scal[1]) < 0 && m.cg_abort) throw std::runtime_error("fallback SR-CG failed");
+    } else {
+      if (m.cg_abort) throw std::runtime_error("SR-CG failed and fallback is disabled");
+      info = -(fallback_iter + 1);
+    }
+  }
+  int imax = 0;
+  for (int i = 1; i < na; ++i)
+    if (std::fabs(x[imax]) < std::fabs(x[i])) imax = i;
+  if (info_out) {
+    const double row[9] = {static_cast<double>(npara), static_cast<double>(na), static_cast<double>(opt_cut),
+                           static_cast<double>(diag_cut), vmax, vmin, x[imax], static_cast<double>(map[imax]),
+                           static_cast<double>(info)};
+    std::copy(row, row + 9, info_out);
+  }
+  for (double v : x)
+    if (!std::isfinite(v)) {
+      if (m.cg_abort) throw std::runtime_error("SR-CG produced non-finite updates");
+      return 1;
+    }
+  std::vector<double> p = mvmc::all_parameters(m);
+  for (int si = 0; si < na; ++si) p[map[si]] += x[si];
+  mvmc::set_all_parameters(m, p);
+  mvmc::sync_modified_parameter(m, true);
+  upload_parameters(c);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int mvmc_b200_create(const char* namelist, const char* initial_def, const mvmc_b200_options* opt,
+                                mvmc_b200_ctx** out) {
+  if (!namelist || !out) return MVMC_B200_EARG;
+  *out = nullptr;
+  mvmc_b200_options o;
+  mvmc_b200_default_options(&o);
+  if (opt) o = *opt;
+  return guarded([&]() {
+    auto* c = new mvmc_b200_ctx();
+    try {
+      build_context(c, namelist, initial_def, o);
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" void mvmc_b200_destroy(mvmc_b200_ctx* ctx) { delete ctx; }
+
+extern "C" int mvmc_b200_dims(const mvmc_b200_ctx* c, int* dims) {
+  if (!c || !dims) return MVMC_B200_EARG;
+  const int v[8] = {c->m.nsite, c->m.ne, c->m.nqp, c->m.nproj(), c->m.npara(), c->S, c->W, c->m.n_orb};
+  std::copy(v, v + 8, dims);
+  return MVMC_B200_OK;
+}
+
+extern "C" int mvmc_b200_get_parameters(const mvmc_b200_ctx* c, double* params, int npara) {
+  if (!c || !params || npara != c->m.npara()) return MVMC_B200_EARG;
+  const std::vector<double> p = mvmc::all_parameters(c->m);
+  std::copy(p.begin(), p.end(), params);
+  return MVMC_B200_OK;
+}
+
+extern "C" int mvmc_b200_set_parameters(mvmc_b200_ctx* c, const double* params, int npara) {
+  if (!c || !params || npara != c->m.npara()) return MVMC_B200_EARG;
+  return guarded([&]() {
+    mvmc::set_all_parameters(c->m, std::vector<double>(params, params + npara));
+    upload_parameters(c);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_sample(mvmc_b200_ctx* c) {
+  if (!c) return MVMC_B200_EARG;
+  return guarded([&]() {
+    int rc = launch_sample(c->dm, c->dw, c->opt.precision, c->stream);
+    if (rc != kOk) return rc;
+    check(cudaStreamSynchronize(c->stream), "sample");
+    c->sampled = true;
+    c->measured = false;
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_get_samples(const mvmc_b200_ctx* c, int64_t* ele_idx, int64_t* ele_cfg, int64_t* ele_num,
+                                     int64_t* proj_cnt, int64_t* counters, int64_t* draws) {
+  if (!c) return MVMC_B200_EARG;
+  return guarded([&]() {
+    const size_t rows = static_cast<size_t>(c->W) * c->S;
+    auto fetch = [&](const int* src, size_t count, int64_t* dst) {
+      if (!dst) return;
+      std::vector<int> tmp(count);
+      check(cudaMemcpy(tmp.data(), src, sizeof(int) * count, cudaMemcpyDeviceToHost), "download samples");
+      for (size_t k = 0; k < count; ++k) dst[k] = tmp[k];
+    };
+    fetch(c->dw.s_idx, rows * c->dm.n, ele_idx);
+    fetch(c->dw.s_cfg, rows * c->dm.ns2, ele_cfg);
+    fetch(c->dw.s_num, rows * c->dm.ns2, ele_num);
+    fetch(c->dw.s_cnt, rows * c->dm.nproj, proj_cnt);
+    if (counters) {
+      std::vector<long long> tmp(static_cast<size_t>(c->W) * 6);
+      check(cudaMemcpy(tmp.data(), c->dw.counter, sizeof(long long) * tmp.size(), cudaMemcpyDeviceToHost), "counters");
+      std::copy(tmp.begin(), tmp.end(), counters);
+    }
+    if (draws) {
+      std::vector<unsigned long long> tmp(c->W);
+      check(cudaMemcpy(tmp.data(), c->dw.draws, sizeof(unsigned long long) * c->W, cudaMemcpyDeviceToHost), "draws");
+      for (int w = 0; w < c->W; ++w) draws[w] = static_cast<int64_t>(tmp[w]);
+    }
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_measure(mvmc_b200_ctx* c, double* energy, double* ho, double* oo) {
+  if (!c) return MVMC_B200_EARG;
+  if (!c->sampled) return MVMC_B200_ESTATE;
+  return guarded([&]() {
+    int rc = do_measure(c);
+    if (rc != kOk) return rc;
+    const int size = c->dm.sr_size;
+    if (energy) std::copy(c->tot.begin(), c->tot.begin() + 5, energy);
+    if (ho) std::copy(c->tot.begin() + 5, c->tot.begin() + 5 + size, ho);
+    if (oo) std::copy(c->tot.begin() + 5 + size, c->tot.begin() + 5 + 3 * size, oo);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_get_o_store(const mvmc_b200_ctx* c, double* o_store, long long count) {
+  if (!c || !o_store) return MVMC_B200_EARG;
+  const long long need = static_cast<long long>(c->W) * c->S * c->dm.sr_size;
+  if (count < need) return MVMC_B200_EARG;
+  return guarded([&]() {
+    check(cudaMemcpy(o_store, c->d_ostore, sizeof(double) * need, cudaMemcpyDeviceToHost), "download O store");
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_get_local_energies(const mvmc_b200_ctx* c, double* e_loc, long long count) {
+  if (!c || !e_loc) return MVMC_B200_EARG;
+  const long long need = static_cast<long long>(c->W) * c->S;
+  if (count < need) return MVMC_B200_EARG;
+  return guarded([&]() {
+    check(cudaMemcpy(e_loc, c->d_eloc, sizeof(double) * need, cudaMemcpyDeviceToHost), "download energies");
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_sr_cg(mvmc_b200_ctx* c, double* sr_info) {
+  if (!c) return MVMC_B200_EARG;
+  return guarded([&]() { return do_sr_cg(c, sr_info); });
+}
+
+extern "C" int mvmc_b200_status(mvmc_b200_ctx* c, unsigned* device_status) {
+  if (!c || !device_status) return MVMC_B200_EARG;
+  return guarded([&]() {
+    check(cudaMemcpy(device_status, c->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_run_opt(const char* namelist, const char* initial_def, const char* out_dir,
+                                 const mvmc_b200_options* opt, int nsteps) {
+  if (!namelist || !out_dir) return MVMC_B200_EARG;
+  mvmc_b200_ctx* c = nullptr;
+  int rc = mvmc_b200_create(namelist, initial_def, opt, &c);
+  if (rc != MVMC_B200_OK) return rc;
+  rc = guarded([&]() {
+    mvmc::Model& m = c->m;
+    if (nsteps > 0) {
+      m.nsr_opt_itr_step = nsteps;
+      m.nsr_opt_itr_smp = std::min(m.nsr_opt_itr_smp, nsteps);
+    }
+    const int window_start = m.nsr_opt_itr_step - m.nsr_opt_itr_smp;
+    std::vector<mvmc::OptPoint> window;
+    bool first_info = true;
+    for (int step = 0; step < m.nsr_opt_itr_step; ++step) {
+      int r = launch_sample(c->dm, c->dw, c->opt.precision, c->stream);
+      if (r != kOk) return r;
+      c->sampled = true;
+      r = do_measure(c);
+      if (r != kOk) return r;
+      const double* t = c->tot.data();
+      mvmc::write_out_row(m, out_dir, step, mvmc::StepEnergy{t[1], t[2], t[3], t[4]});
+      double info[9];
+      const int sr = do_sr_cg(c, info);
+      if (info[1] > 0) {
+        mvmc::SrInfoRow row{static_cast<int>(info[0]), static_cast<int>(info[1]), static_cast<int>(info[2]),
+                            static_cast<int>(info[3]), info[4], info[5], info[6], static_cast<int>(info[7]),
+                            static_cast<int>(info[8])};
+        mvmc::write_srinfo_row(out_dir, m, first_info, row);
+        first_info = false;
+      }
+      if (sr != 0) throw std::runtime_error("SR failed at step " + std::to_string(step));
+      if (step >= window_start) window.push_back({t[1], t[2], mvmc::all_parameters(m)});
+    }
+    mvmc::write_opt_files(m, out_dir, window);
+    return MVMC_B200_OK;
+  });
+  mvmc_b200_destroy(c);
+  return rc;
+}

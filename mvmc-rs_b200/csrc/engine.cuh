@@ -61,4 +61,23 @@ struct DevWalkers {
   int refresh_sweeps;         // mixed path: extra FP64 refresh cadence in sweeps (0 = off)
 };
 
+// Arguments of the cooperative SR-CG solve.
+struct CgArgs {
+  const double* O;     // [ns][na] active sample matrix (rows = samples)
+  const double* mean;  // [na]
+  const double* diag;  // [na]
+  const double* g;     // [na]
+  double* x;           // [na] solution
+  double* r;           // [na] residual
+  double* d;           // [na] direction
+  double* q;           // [na] product / preconditioned residual
+  double* y;           // [ns]
+  double* part;        // [nchunk][na] column partial sums
+  double* red;         // [gridDim] block partials
+  double* scal;        // [8]: delta, status, iterations
+  long long ns;
+  int na, nchunk, max_iter, diag_scale;
+  double inv_w, shift, tol;
+};
+
 }  // namespace mvmcb

@@ -1,0 +1,724 @@
+// K2: resident Metropolis sampler (one CTA per walker).
+//
+// Reproduces vmc_make_sample_real_engine (crates/mvmc-core/src/sampling/driver.rs:175-438)
+// and HostEngine::run_block (sampling/engine.rs:188-476) of AtelierArith/mvmc-rs for the
+// real sz-conserved path, with C's exact draw contract:
+//   get_update_type (candidate.rs:320), make_candidate_hopping / _exchange
+//   (candidate.rs:137,230), update_ele_config / update_proj_cnt / log_proj_ratio
+//   (projection.rs:278,403,418,441), metropolis_decision (metropolis.rs:42-83), the
+//   Pfaffian ratios and rank-2 / rank-4 updates (updates.rs:73,395,588,779,1154,1429),
+//   and the refresh when the accept window exceeds Nsite (engine.rs:454-474).
+// Thread 0 runs the serial Markov-chain logic from the walker's SFMT state in shared
+// memory; the CTA runs the Pfaffian-ratio dots and the inverse updates over all QP
+// planes at once. Planes live in shared memory when they fit, else in the walker's
+// global slice (L2-resident working set).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "pfinv.cuh"
+#include "sfmt.cuh"
+
+namespace mvmcb {
+
+constexpr int kSampThreads = 256;
+
+struct SampLayout {
+  size_t sf, ctl, dctl, idx, cfg, num, cnt, cntn, cntm, pf, pfn, proj, qpw, vec, gj, ws, planes, total;
+};
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+template <typename T>
+__host__ __device__ inline SampLayout samp_layout(const DevModel& m, bool smem_planes, bool smem_ws) {
+  SampLayout L;
+  size_t o = 0;
+  L.sf = o; o = align16(o + sizeof(uint32_t) * kSfmtN32);
+  L.ctl = o; o = align16(o + sizeof(int) * 32);
+  L.dctl = o; o = align16(o + sizeof(double) * 8);
+  L.idx = o; o = align16(o + sizeof(int) * m.n);
+  L.cfg = o; o = align16(o + sizeof(int) * m.ns2);
+  L.num = o; o = align16(o + sizeof(int) * m.ns2);
+  L.cnt = o; o = align16(o + sizeof(int) * (m.nproj + 1));
+  L.cntn = o; o = align16(o + sizeof(int) * (m.nproj + 1));
+  L.cntm = o; o = align16(o + sizeof(int) * (m.nproj + 1));
+  L.pf = o; o = align16(o + sizeof(double) * m.nqp);
+  L.pfn = o; o = align16(o + sizeof(double) * m.nqp);
+  L.proj = o; o = align16(o + sizeof(double) * (m.nproj + 1));
+  L.qpw = o; o = align16(o + sizeof(double) * m.nqp);
+  L.vec = o; o = align16(o + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n + sizeof(double) * 8 * m.nqp);
+  L.gj = o; o = align16(o + gj_shared_bytes<double>(m.n));
+  L.ws = o;
+  if (smem_ws) o = align16(o + sizeof(double) * static_cast<size_t>(m.n) * m.n);
+  L.planes = o;
+  if (smem_planes) o = align16(o + sizeof(T) * static_cast<size_t>(m.nqp) * m.n * m.n);
+  L.total = o;
+  return L;
+}
+
+// Control slots in shared memory.
+enum Ctl {
+  cSkip = 0, cType, cMi, cRi, cRj, cS, cMj, cT, cMsa, cMsb, cAccept, cRefresh, cInfo, cNacc,
+  cBurn, cAttempt, cStop
+};
+enum DCtl { dLogIp = 0, dLogIpNew = 1 };
+
+template <typename T>
+struct WalkerSmem {
+  uint32_t* sf;
+  int* ctl;
+  double* dctl;
+  int *idx, *cfg, *num, *cnt, *cntn, *cntm;
+  double *pf, *pfn, *proj, *qpw;
+  T* vec;          // [nqp][4][n]
+  double* pscal;   // [nqp][8] per-plane scalars
+  GJShared<double> gj;
+  double* ws;      // FP64 refresh workspace (n*n)
+  T* planes;       // [nqp][n][n]
+};
+
+__device__ __forceinline__ int rs_of(const DevModel& m, const int* idx, int k) {
+  return idx[k] + (k >= m.ne ? m.ns : 0);
+}
+
+template <typename T>
+__device__ __forceinline__ T slater_at(const DevModel& m, int q, int r1, int r2);
+template <>
+__device__ __forceinline__ double slater_at<double>(const DevModel& m, int q, int r1, int r2) {
+  return __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + r1) * m.ns2 + r2);
+}
+template <>
+__device__ __forceinline__ float slater_at<float>(const DevModel& m, int q, int r1, int r2) {
+  return __ldg(m.slater32 + (static_cast<size_t>(q) * m.ns2 + r1) * m.ns2 + r2);
+}
+
+// ---- projection counters --------------------------------------------------------------
+__device__ void make_proj_cnt_serial(const DevModel& m, const int* num, int* cnt) {
+  for (int k = 0; k < m.nproj; ++k) cnt[k] = 0;
+  for (int ri = 0; ri < m.ns; ++ri) {
+    const int g = m.gutz_idx[ri];
+    if (m.n_gutz > 0 && g >= 0 && g < m.nproj) cnt[g] += num[ri] * num[ri + m.ns];
+  }
+  if (m.n_jast > 0)
+    for (int ri = 0; ri < m.ns; ++ri) {
+      const int xi = num[ri] + num[ri + m.ns] - 1;
+      if (xi == 0) continue;
+      for (int rj = ri + 1; rj < m.ns; ++rj) {
+        const int j = __ldg(m.jast_idx + ri * m.ns + rj);
+        if (j < 0) continue;
+        const int xj = num[rj] + num[rj + m.ns] - 1;
+        if (m.n_gutz + j < m.nproj) cnt[m.n_gutz + j] += xi * xj;
+      }
+    }
+}
+
+// update_proj_cnt by one warp; `num` accessor gives the occupation after the move.
+template <typename NumFn>
+__device__ void update_proj_cnt_warp(const DevModel& m, int ri, int rj, int* cnew, const int* cold,
+                                     NumFn num) {
+  const int lane = threadIdx.x & 31;
+  for (int k = lane; k < m.nproj; k += 32) cnew[k] = cold[k];
+  __syncwarp();
+  if (ri == rj) return;
+  const int ns = m.ns;
+  if (lane == 0 && m.n_gutz > 0) {
+    const int gi = m.gutz_idx[ri], gj = m.gutz_idx[rj];
+    if (gi >= 0 && gi < m.nproj) atomicAdd(cnew + gi, -(num(ri) + num(ri + ns)));
+    if (gj >= 0 && gj < m.nproj) atomicAdd(cnew + gj, num(rj) * num(rj + ns));
+  }
+  if (m.n_jast > 0) {
+    const int off = m.n_gutz;
+    auto jidx = [&](int a, int b) { return __ldg(m.jast_idx + min(a, b) * ns + max(a, b)); };
+    if (lane == 0) {
+      const int ij = jidx(ri, rj);
+      if (ij >= 0) atomicAdd(cnew + off + ij, (num(ri) + num(ri + ns)) - (num(rj) + num(rj + ns)) + 1);
+    }
+    for (int rk = lane; rk < ns; rk += 32) {
+      if (rk == ri || rk == rj) continue;
+      const int xk = num(rk) + num(rk + ns) - 1;
+      if (xk == 0) continue;
+      const int ik = jidx(ri, rk), jk = jidx(rj, rk);
+      if (ik >= 0) atomicAdd(cnew + off + ik, -xk);
+      if (jk >= 0) atomicAdd(cnew + off + jk, xk);
+    }
+  }
+  __syncwarp();
+}
+
+// ---- CalculateMAll on every plane (CTA-wide); returns 0 ok, else the first failure -------
+template <typename T>
+__device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status) {
+  const int n = m.n;
+  int info = 0;
+  for (int q = 0; q < m.nqp; ++q) {
+    double* A = s.ws ? s.ws : reinterpret_cast<double*>(s.planes + static_cast<size_t>(q) * n * n);
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+      const int i = k / n, j = k - i * n;
+      A[k] = __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + rs_of(m, s.idx, i)) * m.ns2 +
+                   rs_of(m, s.idx, j));
+    }
+    __syncthreads();
+    double pfv;
+    int st;
+    gj_pfinv<double>(A, n, n, s.gj, pfv, st);
+    if (s.ws) {
+      T* P = s.planes + static_cast<size_t>(q) * n * n;
+      for (int k = threadIdx.x; k < n * n; k += blockDim.x) P[k] = static_cast<T>(A[k]);
+      __syncthreads();
+    }
+    if (st != 0) {
+      info = st;
+      break;
+    }
+    if (threadIdx.x == 0) s.pf[q] = pfv;
+  }
+  __syncthreads();
+  return info;
+}
+
+__device__ __forceinline__ double log_ip_of(const DevModel& m, const double* pf, const double* qpw) {
+  double ip = 0.0;
+  for (int q = 0; q < m.nqp; ++q) ip += qpw[q] * pf[q];
+  return log(fabs(ip));
+}
+
+// ---- Pfaffian ratio of a hop: pf_new[q] = -pf[q]·Σ_j InvM[q][msa][j]·S_q[rsa][rs_j] --------
+template <typename T>
+__device__ void ratio_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa) {
+  const int n = m.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int rsa = rs_of(m, s.idx, msa);
+  for (int q = warp; q < m.nqp; q += nwarp) {
+    const T* row = s.planes + (static_cast<size_t>(q) * n + msa) * n;
+    T r = T(0);
+    for (int j = lane; j < n; j += 32) r += row[j] * slater_at<T>(m, q, rsa, rs_of(m, s.idx, j));
+    r = warp_sum(r);
+    if (lane == 0) s.pfn[q] = -static_cast<double>(r) * s.pf[q];
+  }
+}
+
+// ---- rank-2 update of an accepted hop (update_one_real) -----------------------------------
+template <typename T>
+__device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa) {
+  const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
+  const int rsa = rs_of(m, s.idx, msa);
+  T* vec = s.vec;  // [q][0]=slt, [1]=vec1, [2]=vec2
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, i = k - q * n;
+    vec[(q * 4 + 0) * n + i] = slater_at<T>(m, q, rsa, rs_of(m, s.idx, i));
+  }
+  __syncthreads();
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, j = k - q * n;
+    const T* P = s.planes + static_cast<size_t>(q) * n * n;
+    const T* slt = vec + (q * 4 + 0) * n;
+    T acc = T(0);
+    for (int i = 0; i < n; ++i) acc += -P[i * n + j] * slt[i];
+    vec[(q * 4 + 1) * n + j] = acc;
+  }
+  __syncthreads();
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, j = k - q * n;
+    const T tmp = vec[(q * 4 + 1) * n + msa];
+    const T ia = T(-1) / tmp;
+    vec[(q * 4 + 2) * n + j] = s.planes[(static_cast<size_t>(q) * n + msa) * n + j] * ia;
+    if (j == 0) s.pf[q] *= -static_cast<double>(tmp);
+  }
+  __syncthreads();
+  const size_t total = static_cast<size_t>(nq) * n * n;
+  for (size_t k = tid; k < total; k += nt) {
+    const int q = static_cast<int>(k / (static_cast<size_t>(n) * n));
+    const int r = static_cast<int>(k - static_cast<size_t>(q) * n * n);
+    const int i = r / n, j = r - i * n;
+    const T* v1 = vec + (q * 4 + 1) * n;
+    const T* v2 = vec + (q * 4 + 2) * n;
+    T x = s.planes[k] + (v1[i] * v2[j] - v1[j] * v2[i]);
+    if (j == msa) x -= v2[i];
+    if (i == msa) x += v2[j];
+    s.planes[k] = x;
+  }
+  __syncthreads();
+}
+
+// ---- exchange ratio (two_ratio_real, updates.rs:1539-1622) --------------------------------
+template <typename T>
+__device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, int msb) {
+  const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  const int rsa = rs_of(m, s.idx, msa), rsb = rs_of(m, s.idx, msb);
+  T* vec = s.vec;  // [0]=va, [1]=vb, [2]=inv·va
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, i = k - q * n;
+    const int ri = rs_of(m, s.idx, i);
+    vec[(q * 4 + 0) * n + i] = slater_at<T>(m, q, rsa, ri);
+    vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
+  }
+  __syncthreads();
+  for (int row = warp; row < nq * n; row += nwarp) {
+    const int q = row / n, i = row - q * n;
+    const T* P = s.planes + (static_cast<size_t>(q) * n + i) * n;
+    const T* va = vec + (q * 4 + 0) * n;
+    T t = T(0);
+    for (int j = lane; j < n; j += 32) t += P[j] * va[j];
+    t = warp_sum(t);
+    if (lane == 0) vec[(q * 4 + 2) * n + i] = t;
+  }
+  __syncthreads();
+  for (int q = warp; q < nq; q += nwarp) {
+    const T* P = s.planes + static_cast<size_t>(q) * n * n;
+    const T* va = vec + (q * 4 + 0) * n;
+    const T* vb = vec + (q * 4 + 1) * n;
+    const T* ia = vec + (q * 4 + 2) * n;
+    T pa = 0, pb = 0, qa = 0, qb = 0, bma = 0;
+    for (int i = lane; i < n; i += 32) {
+      pa += P[msa * n + i] * va[i];
+      pb += P[msb * n + i] * va[i];
+      qa += P[msa * n + i] * vb[i];
+      qb += P[msb * n + i] * vb[i];
+      bma += vb[i] * ia[i];
+    }
+    pa = warp_sum(pa);
+    pb = warp_sum(pb);
+    qa = warp_sum(qa);
+    qb = warp_sum(qb);
+    bma = warp_sum(bma);
+    if (lane == 0) {
+      const T iab = P[msa * n + msb];
+      const T ratio = iab * vb[msa] + iab * bma + pa * qb - pb * qa;
+      s.pfn[q] = static_cast<double>(ratio) * s.pf[q];
+    }
+  }
+}
+
+// ---- rank-4 update of an accepted exchange (update_two_real, updates.rs:1429-1505) --------
+template <typename T>
+__device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, int msb,
+                                    int rsa_old, int rsb_old) {
+  const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  const int rsa = rs_of(m, s.idx, msa), rsb = rs_of(m, s.idx, msb);
+  T* vec = s.vec;  // [0]=vs, [1]=vt, [2]=vp, [3]=vq
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, i = k - q * n;
+    const int ri = rs_of(m, s.idx, i);
+    vec[(q * 4 + 0) * n + i] = (i == msb) ? slater_at<T>(m, q, rsa_old, rsb_old) : slater_at<T>(m, q, rsa, ri);
+    vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
+  }
+  __syncthreads();
+  for (int row = warp; row < nq * n; row += nwarp) {
+    const int q = row / n, i = row - q * n;
+    const T* P = s.planes + (static_cast<size_t>(q) * n + i) * n;
+    const T* vs = vec + (q * 4 + 0) * n;
+    const T* vt = vec + (q * 4 + 1) * n;
+    T p = T(0), r = T(0);
+    for (int j = lane; j < n; j += 32) {
+      p += P[j] * vs[j];
+      r += P[j] * vt[j];
+    }
+    p = warp_sum(p);
+    r = warp_sum(r);
+    if (lane == 0) {
+      vec[(q * 4 + 2) * n + i] = p;
+      vec[(q * 4 + 3) * n + i] = r;
+    }
+  }
+  __syncthreads();
+  double* sc = s.pscal;  // per plane: a b c d e f idet det
+  for (int q = warp; q < nq; q += nwarp) {
+    const T* vt = vec + (q * 4 + 1) * n;
+    const T* vp = vec + (q * 4 + 2) * n;
+    const T* vq = vec + (q * 4 + 3) * n;
+    T bma = T(0);
+    for (int i = lane; i < n; i += 32) bma += vt[i] * vp[i];
+    bma = warp_sum(bma);
+    if (lane == 0) {
+      const T* P = s.planes + static_cast<size_t>(q) * n * n;
+      const T iab = P[msa * n + msb];
+      const T ratio = iab * vt[msa] + iab * bma + vp[msa] * vq[msb] - vp[msb] * vq[msa];
+      s.pf[q] *= static_cast<double>(ratio);
+      const T a = -vp[msa], b = vp[msb], c = vq[msa], d = -vq[msb];
+      const T e = -bma - vt[msa], f = iab;
+      const T det = a * d - b * c - e * f;
+      const T idet = T(1) / det;
+      double* o = sc + q * 8;
+      o[0] = a; o[1] = b; o[2] = c; o[3] = d; o[4] = e; o[5] = f; o[6] = idet; o[7] = det;
+    }
+  }
+  __syncthreads();
+  // vs <- idet·InvM[msa][:], vt <- idet·InvM[msb][:]
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, i = k - q * n;
+    const T idet = static_cast<T>(sc[q * 8 + 6]);
+    const T* P = s.planes + static_cast<size_t>(q) * n * n;
+    vec[(q * 4 + 0) * n + i] = idet * P[msa * n + i];
+    vec[(q * 4 + 1) * n + i] = idet * P[msb * n + i];
+  }
+  __syncthreads();
+  const size_t total = static_cast<size_t>(nq) * n * n;
+  for (size_t k = tid; k < total; k += nt) {
+    const int q = static_cast<int>(k / (static_cast<size_t>(n) * n));
+    const int r = static_cast<int>(k - static_cast<size_t>(q) * n * n);
+    const int i = r / n, j = r - i * n;
+    const double* o = sc + q * 8;
+    const T a = o[0], b = o[1], c = o[2], d = o[3], e = o[4], f = o[5], idet = o[6], det = o[7];
+    const T* vs = vec + (q * 4 + 0) * n;
+    const T* vt = vec + (q * 4 + 1) * n;
+    const T* vp = vec + (q * 4 + 2) * n;
+    const T* vq = vec + (q * 4 + 3) * n;
+    const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
+    const T pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
+    T x = s.planes[k] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
+                         d * (pi * sj - pj * si) + e * det * (si * tj - sj * ti) +
+                         f * idet * (pi * qj - qi * pj));
+    if (j == msa) x += -c * ti - d * si - f * idet * qi;
+    if (j == msb) x += -a * ti - b * si + f * idet * pi;
+    if (i == msa) x += c * tj + d * sj + f * idet * qj;
+    if (i == msb) x += a * tj + b * sj - f * idet * pj;
+    if (i == msa && j == msb) x += f * idet;
+    if (i == msb && j == msa) x -= f * idet;
+    s.planes[k] = x;
+  }
+  __syncthreads();
+}
+
+// ---- serial helpers for thread 0 ------------------------------------------------------------
+__device__ __forceinline__ void move_electron(const DevModel& m, int* idx, int* cfg, int* num, int mi,
+                                              int ri, int rj, int sp) {
+  const int msa = mi + sp * m.ne, ro = ri + sp * m.ns, rn = rj + sp * m.ns;
+  idx[msa] = rj;
+  cfg[ro] = -1;
+  cfg[rn] = mi;
+  num[ro] = 0;
+  num[rn] = 1;
+}
+__device__ __forceinline__ void revert_electron(const DevModel& m, int* idx, int* cfg, int* num, int mi,
+                                                int ri, int rj, int sp) {
+  const int msa = mi + sp * m.ne, ro = ri + sp * m.ns, rn = rj + sp * m.ns;
+  idx[msa] = ri;
+  cfg[ro] = mi;
+  cfg[rn] = -1;
+  num[ro] = 1;
+  num[rn] = 0;
+}
+
+__device__ void make_initial_sample_dev(const DevModel& m, SfmtRef& rng, int* idx, int* cfg, int* num,
+                                        int* cnt) {
+  for (int k = 0; k < m.n; ++k) idx[k] = -1;
+  for (int k = 0; k < m.ns2; ++k) cfg[k] = -1;
+  for (int si = 0; si < 2; ++si)
+    for (int mi = 0; mi < m.ne; ++mi) {
+      int guard = 0;
+      while (true) {
+        const int ri = static_cast<int>(rng.mod(m.ns));
+        if (cfg[ri + si * m.ns] == -1) {
+          cfg[ri + si * m.ns] = mi;
+          idx[mi + si * m.ne] = ri;
+          break;
+        }
+        if (++guard > (1 << 24)) break;  // unreachable for ne <= nsite
+      }
+    }
+  for (int r = 0; r < m.ns2; ++r) num[r] = cfg[r] < 0 ? 0 : 1;
+  make_proj_cnt_serial(m, num, cnt);
+}
+
+template <typename T, bool kSmemPlanes, bool kSmemWs>
+__global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers w) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int wk = blockIdx.x;
+  const int tid = threadIdx.x;
+  const SampLayout L = samp_layout<T>(m, kSmemPlanes, kSmemWs);
+  WalkerSmem<T> s;
+  s.sf = reinterpret_cast<uint32_t*>(smem + L.sf);
+  s.ctl = reinterpret_cast<int*>(smem + L.ctl);
+  s.dctl = reinterpret_cast<double*>(smem + L.dctl);
+  s.idx = reinterpret_cast<int*>(smem + L.idx);
+  s.cfg = reinterpret_cast<int*>(smem + L.cfg);
+  s.num = reinterpret_cast<int*>(smem + L.num);
+  s.cnt = reinterpret_cast<int*>(smem + L.cnt);
+  s.cntn = reinterpret_cast<int*>(smem + L.cntn);
+  s.cntm = reinterpret_cast<int*>(smem + L.cntm);
+  s.pf = reinterpret_cast<double*>(smem + L.pf);
+  s.pfn = reinterpret_cast<double*>(smem + L.pfn);
+  s.proj = reinterpret_cast<double*>(smem + L.proj);
+  s.qpw = reinterpret_cast<double*>(smem + L.qpw);
+  s.vec = reinterpret_cast<T*>(smem + L.vec);
+  s.pscal = reinterpret_cast<double*>(smem + L.vec + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n);
+  s.gj = gj_carve<double>(smem + L.gj, m.n);
+  const size_t nn = static_cast<size_t>(m.n) * m.n;
+  if (kSmemWs) s.ws = reinterpret_cast<double*>(smem + L.ws);
+  else s.ws = (sizeof(T) == sizeof(double)) ? nullptr : w.ws64 + static_cast<size_t>(wk) * nn;
+  s.planes = kSmemPlanes ? reinterpret_cast<T*>(smem + L.planes)
+                         : reinterpret_cast<T*>(w.inv) + static_cast<size_t>(wk) * m.nqp * nn;
+
+  // ---- load the walker ----
+  for (int k = tid; k < kSfmtN32; k += blockDim.x) s.sf[k] = w.sfmt[static_cast<size_t>(wk) * kSfmtN32 + k];
+  for (int k = tid; k < m.n; k += blockDim.x) s.idx[k] = w.ele_idx[static_cast<size_t>(wk) * m.n + k];
+  for (int k = tid; k < m.ns2; k += blockDim.x) {
+    s.cfg[k] = w.ele_cfg[static_cast<size_t>(wk) * m.ns2 + k];
+    s.num[k] = w.ele_num[static_cast<size_t>(wk) * m.ns2 + k];
+  }
+  for (int k = tid; k < m.nproj; k += blockDim.x) {
+    s.cnt[k] = w.proj_cnt[static_cast<size_t>(wk) * m.nproj + k];
+    s.proj[k] = m.proj[k];
+  }
+  for (int k = tid; k < m.nqp; k += blockDim.x) s.qpw[k] = m.qpw[k];
+  __shared__ int sf_idx;
+  __shared__ unsigned long long sf_draws;
+  if (tid == 0) {
+    sf_idx = w.sfmt_idx[wk];
+    sf_draws = w.draws[wk];
+    s.ctl[cBurn] = w.burn[wk];
+  }
+  __syncthreads();
+  SfmtRef rng{s.sf, &sf_idx, &sf_draws};
+  const int n = m.n, ns = m.ns, ne = m.ne;
+  bool burn = s.ctl[cBurn] != 0;
+
+  // ---- initial configuration (makeInitialSample with the C retry rule) ----
+  auto initial = [&]() {
+    for (int attempt = 1; attempt <= 101; ++attempt) {
+      if (tid == 0) make_initial_sample_dev(m, rng, s.idx, s.cfg, s.num, s.cnt);
+      __syncthreads();
+      const int info = calc_m_all_dev<T>(m, s, w.status);
+      if (attempt > 100) {
+        if (tid == 0) atomicOr(w.status, kDevInitLoops);
+        return;
+      }
+      if (info <= 0) return;
+    }
+  };
+  if (!burn) initial();
+  calc_m_all_dev<T>(m, s, w.status);
+  if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
+  __syncthreads();
+  if (!isfinite(s.dctl[dLogIp])) {
+    initial();
+    calc_m_all_dev<T>(m, s, w.status);
+    if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
+    burn = false;
+    __syncthreads();
+  }
+  const int S = m.saved;
+  const int n_out = burn ? S + 1 : m.warmup + S;
+  const int n_in = m.interval * max(1, ns);
+  long long counter[6] = {0, 0, 0, 0, 0, 0};
+  int n_acc_win = 0;
+  const int refresh_every = (sizeof(T) == sizeof(float) && w.refresh_sweeps > 0) ? w.refresh_sweeps * max(1, ns) : 0;
+  long long since_refresh = 0;
+
+  long long proposal = 0;
+  for (int out = 0; out < n_out; ++out) {
+    for (int step = 0; step < n_in; ++step, ++proposal) {
+      // Candidate slots alternate between two banks: a skipped proposal has no later
+      // barrier, so the next proposal must not overwrite the bank still being read.
+      int* const cc = s.ctl + ((proposal & 1) ? 16 : 0);
+      // --- candidate (thread 0) ---
+      if (tid == 0) {
+        int type;
+        switch (m.nex_path) {
+          case 0: type = 0; break;
+          case 1: type = rng.real2() < 0.5 ? 1 : 0; break;
+          case 2: type = 1; break;
+          default: type = 3;
+        }
+        int skip = 1;
+        if (type == 0) {
+          counter[0]++;
+          const int mi = static_cast<int>(rng.mod(ne));
+          const int sp = rng.real2() < 0.5 ? 0 : 1;
+          const int ri = s.idx[mi + sp * ne];
+          int rj = 0, icnt = 0;
+          bool reject = false;
+          const int icnt_max = ns * ns;
+          while (true) {
+            rj = static_cast<int>(rng.mod(ns));
+            if (icnt > icnt_max) {
+              reject = true;
+              break;
+            }
+            ++icnt;
+            if (s.cfg[rj + sp * ns] == -1) break;
+          }
+          if (!reject) {
+            move_electron(m, s.idx, s.cfg, s.num, mi, ri, rj, sp);
+            cc[cMi] = mi; cc[cRi] = ri; cc[cRj] = rj; cc[cS] = sp;
+            cc[cMsa] = mi + sp * ne;
+            skip = 0;
+          }
+        } else if (type == 1) {
+          counter[2]++;
+          bool single = false;
+          for (int r = 0; r < ns; ++r)
+            if (s.num[r] + s.num[r + ns] == 1) {
+              single = true;
+              break;
+            }
+          if (single) {
+            int mi, sp, ri, mj, rj;
+            // The C loops are unbounded; a partner always exists for sz-balanced
+            // configurations. The bound only turns a malformed input into a status bit.
+            constexpr int kLoopBound = 1 << 22;
+            int guard = 0;
+            while (true) {
+              mi = static_cast<int>(rng.mod(ne));
+              sp = rng.real2() < 0.5 ? 0 : 1;
+              ri = s.idx[mi + sp * ne];
+              if (s.cfg[ri + (1 - sp) * ns] == -1 || ++guard > kLoopBound) break;
+            }
+            const int t = 1 - sp;
+            while (guard <= kLoopBound) {
+              mj = static_cast<int>(rng.mod(ne));
+              rj = s.idx[mj + t * ne];
+              if (s.cfg[rj + sp * ns] == -1 || ++guard > kLoopBound) break;
+            }
+            if (guard > kLoopBound) {
+              atomicOr(w.status, kDevCandidateLoop);  // skip stays 1: no move is made
+            } else {
+              move_electron(m, s.idx, s.cfg, s.num, mi, ri, rj, sp);
+              move_electron(m, s.idx, s.cfg, s.num, mj, rj, ri, t);
+              cc[cMi] = mi; cc[cRi] = ri; cc[cRj] = rj; cc[cS] = sp;
+              cc[cMj] = mj; cc[cT] = t;
+              cc[cMsa] = mi + sp * ne;
+              cc[cMsb] = mj + t * ne;
+              skip = 0;
+            }
+          }
+        }
+        cc[cType] = type;
+        cc[cSkip] = skip;
+      }
+      __syncthreads();
+      if (cc[cSkip]) continue;
+      const int type = cc[cType];
+      const int ri = cc[cRi], rj = cc[cRj], sp = cc[cS], msa = cc[cMsa];
+      // --- projection counters (warp 0) and Pfaffian ratios (CTA) ---
+      if (type == 0) {
+        if (tid < 32) update_proj_cnt_warp(m, ri, rj, s.cntn, s.cnt, [&](int k) { return s.num[k]; });
+        ratio_hop_dev<T>(m, s, msa);
+      } else {
+        const int t = cc[cT];
+        if (tid < 32) {
+          // first move uses the occupation before the partner's move
+          const int a = rj + t * ns, b = ri + t * ns;
+          auto num_mid = [&](int k) { return k == a ? 1 : (k == b ? 0 : s.num[k]); };
+          update_proj_cnt_warp(m, ri, rj, s.cntm, s.cnt, num_mid);
+          update_proj_cnt_warp(m, rj, ri, s.cntn, s.cntm, [&](int k) { return s.num[k]; });
+        }
+        ratio_exchange_dev<T>(m, s, msa, cc[cMsb]);
+      }
+      __syncthreads();
+      // --- Metropolis (thread 0) ---
+      if (tid == 0) {
+        double ip = 0.0;
+        for (int q = 0; q < m.nqp; ++q) ip += s.qpw[q] * s.pfn[q];
+        const double lip_new = log(fabs(ip));
+        double dproj = 0.0;
+        for (int k = 0; k < m.nproj; ++k) dproj += s.proj[k] * static_cast<double>(s.cntn[k] - s.cnt[k]);
+        double wgt = exp(2.0 * ((dproj + 0.0 + lip_new) - s.dctl[dLogIp]));
+        if (!isfinite(wgt)) wgt = -1.0;
+        const double u = rng.real2();
+        const int acc = wgt > u ? 1 : 0;
+        if (acc) {
+          for (int k = 0; k < m.nproj; ++k) s.cnt[k] = s.cntn[k];
+          s.dctl[dLogIp] = lip_new;
+          ++n_acc_win;
+          counter[type == 0 ? 1 : 3]++;
+        } else if (type == 0) {
+          revert_electron(m, s.idx, s.cfg, s.num, cc[cMi], ri, rj, sp);
+        } else {
+          revert_electron(m, s.idx, s.cfg, s.num, cc[cMj], rj, ri, cc[cT]);
+          revert_electron(m, s.idx, s.cfg, s.num, cc[cMi], ri, rj, sp);
+        }
+        cc[cAccept] = acc;
+        ++since_refresh;
+        int refresh = 0;
+        if (n_acc_win > ns) {
+          refresh = 1;
+          n_acc_win = 0;
+        } else if (refresh_every > 0 && since_refresh >= refresh_every) {
+          refresh = 2;  // extra FP64 refresh of the mixed path (does not reset the C window)
+        }
+        if (refresh) since_refresh = 0;
+        cc[cRefresh] = refresh;
+      }
+      __syncthreads();
+      if (cc[cAccept]) {
+        if (type == 0) {
+          update_hop_dev<T>(m, s, msa);
+        } else {
+          update_exchange_dev<T>(m, s, msa, cc[cMsb], ri + sp * ns, rj + cc[cT] * ns);
+        }
+      }
+      if (cc[cRefresh]) {
+        const int info = calc_m_all_dev<T>(m, s, w.status);
+        if (tid == 0 && info == 0 && cc[cRefresh] == 1) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
+        if (tid == 0 && info == 0 && cc[cRefresh] == 2) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
+        __syncthreads();
+      }
+    }
+    if (out + S >= n_out) {
+      const size_t sample = static_cast<size_t>(wk) * S + (out + S - n_out);
+      for (int k = tid; k < n; k += blockDim.x) w.s_idx[sample * n + k] = s.idx[k];
+      for (int k = tid; k < m.ns2; k += blockDim.x) {
+        w.s_cfg[sample * m.ns2 + k] = s.cfg[k];
+        w.s_num[sample * m.ns2 + k] = s.num[k];
+      }
+      for (int k = tid; k < m.nproj; k += blockDim.x) w.s_cnt[sample * m.nproj + k] = s.cnt[k];
+    }
+  }
+  __syncthreads();
+  // ---- store the walker (the final configuration is the burn-in state of the next step) ----
+  for (int k = tid; k < kSfmtN32; k += blockDim.x) w.sfmt[static_cast<size_t>(wk) * kSfmtN32 + k] = s.sf[k];
+  for (int k = tid; k < n; k += blockDim.x) w.ele_idx[static_cast<size_t>(wk) * n + k] = s.idx[k];
+  for (int k = tid; k < m.ns2; k += blockDim.x) {
+    w.ele_cfg[static_cast<size_t>(wk) * m.ns2 + k] = s.cfg[k];
+    w.ele_num[static_cast<size_t>(wk) * m.ns2 + k] = s.num[k];
+  }
+  for (int k = tid; k < m.nproj; k += blockDim.x) w.proj_cnt[static_cast<size_t>(wk) * m.nproj + k] = s.cnt[k];
+  for (int k = tid; k < m.nqp; k += blockDim.x) w.pf[static_cast<size_t>(wk) * m.nqp + k] = s.pf[k];
+  if (tid == 0) {
+    w.sfmt_idx[wk] = sf_idx;
+    w.draws[wk] = sf_draws;
+    w.burn[wk] = 1;
+    for (int k = 0; k < 6; ++k) w.counter[static_cast<size_t>(wk) * 6 + k] = counter[k];
+  }
+}
+
+// ---- host launch ---------------------------------------------------------------------------
+int smem_limit_bytes();
+
+template <typename T, bool kSmemPlanes, bool kSmemWs>
+int launch_sample_t(const DevModel& m, const DevWalkers& w, cudaStream_t stream) {
+  const size_t smem = samp_layout<T>(m, kSmemPlanes, kSmemWs).total;
+  MVMCB_CUDA(cudaFuncSetAttribute(k_sample<T, kSmemPlanes, kSmemWs>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_sample<T, kSmemPlanes, kSmemWs><<<w.W, kSampThreads, smem, stream>>>(m, w);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+// Shared-memory residency: planes (and for FP32 the FP64 refresh workspace) in shared
+// memory when they fit the per-block opt-in limit.
+bool sample_planes_in_smem(const DevModel& m, int precision, int limit) {
+  if (precision == 32) return samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit) ||
+                              samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit);
+  return samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit);
+}
+
+int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStream_t stream) {
+  int dev = 0, limit = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (precision == 32) {
+    if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit))
+      return launch_sample_t<float, true, true>(m, w, stream);
+    if (samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit))
+      return launch_sample_t<float, true, false>(m, w, stream);
+    return launch_sample_t<float, false, false>(m, w, stream);
+  }
+  if (samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit))
+    return launch_sample_t<double, true, false>(m, w, stream);
+  return launch_sample_t<double, false, false>(m, w, stream);
+}
+
+}  // namespace mvmcb

@@ -19,7 +19,7 @@ EXPORTS = [
     "mvmc_b200_get_parameters", "mvmc_b200_set_parameters", "mvmc_b200_sample",
     "mvmc_b200_get_samples", "mvmc_b200_measure", "mvmc_b200_get_o_store",
     "mvmc_b200_get_local_energies", "mvmc_b200_sr_cg", "mvmc_b200_status", "mvmc_b200_run_opt",
-    "mvmc_b200_last_error",
+    "mvmc_b200_last_error", "mvmc_b200_cg_solve",
 ]
 
 
@@ -70,6 +70,22 @@ def pfinv_batch_mixed(x, sizes, precision=64):
     _check(lib().mvmc_b200_pfinv_batch_mixed(_ptr(x), _ptr(sizes), planes, precision, _ptr(pf),
                                              _ptr(inv), _ptr(st)), "pfinv_batch_mixed")
     return pf, inv, st
+
+
+def cg_solve(samples, mean, diag, g, inv_w, shift, tol, max_iter, diag_scale=False):
+    """SR-CG on fixed operands; samples is [ns][na]."""
+    samples = np.ascontiguousarray(samples, dtype=np.float64)
+    na = len(mean)
+    ns = samples.size // na
+    x = np.zeros(na)
+    st = ctypes.c_longlong()
+    _check(lib().mvmc_b200_cg_solve(_ptr(samples), ctypes.c_longlong(ns), na,
+                                    _ptr(np.ascontiguousarray(mean, dtype=np.float64)),
+                                    _ptr(np.ascontiguousarray(diag, dtype=np.float64)),
+                                    _ptr(np.ascontiguousarray(g, dtype=np.float64)),
+                                    ctypes.c_double(inv_w), ctypes.c_double(shift), ctypes.c_double(tol),
+                                    max_iter, int(diag_scale), _ptr(x), ctypes.byref(st)), "cg_solve")
+    return st.value, x
 
 
 def default_options(**kw):

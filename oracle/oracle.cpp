@@ -1301,6 +1301,46 @@ int oracle_physcal_samples(const char* namelist, const char* zqp_opt, long long 
   }
 }
 
+int oracle_opt_step1_walkers(const char* namelist, const char* initial_def, int walkers,
+                             long long seed, int64_t* ele_idx, int64_t* proj_cnt, int64_t* counters,
+                             int64_t* draws, double* energy, double* ho, double* oo, double* ostore,
+                             char* err, int err_len) {
+  try {
+    mvmc::Model m = mvmc::read_expert(namelist);
+    if (m.nsrcg == 0) m.nsrcg = 1;
+    std::vector<orc::Walker> ws(std::max(1, walkers));
+    orc::seed_walkers(m, ws, seed >= 0 ? seed : m.rnd_seed);
+    if (initial_def && *initial_def) {
+      std::string why;
+      if (!mvmc::read_para_triples(m, initial_def, &why)) throw std::runtime_error("initial.def: " + why);
+    }
+    mvmc::sync_modified_parameter(m, true);
+    mvmc::init_qp_weight(m);
+    std::vector<orc::Accum> acc;
+    orc::Accum tot;
+    orc::sample_and_measure(m, ws, acc, tot);
+    const int n = m.nsize(), size = m.sr_size(), S = m.nvmc_sample, np = m.nproj();
+    for (size_t w = 0; w < ws.size(); ++w) {
+      std::copy(ws[w].s_idx.begin(), ws[w].s_idx.end(), ele_idx + w * S * n);
+      std::copy(ws[w].s_cnt.begin(), ws[w].s_cnt.end(), proj_cnt + w * S * np);
+      for (int k = 0; k < 6; ++k) counters[w * 6 + k] = ws[w].counter[k];
+      draws[w] = static_cast<int64_t>(ws[w].rng.draws);
+      std::copy(acc[w].store.begin(), acc[w].store.end(), ostore + w * S * size);
+    }
+    energy[0] = tot.wc;
+    energy[1] = tot.etot;
+    energy[2] = tot.etot2;
+    energy[3] = tot.sztot;
+    energy[4] = tot.sztot2;
+    std::copy(tot.ho.begin(), tot.ho.end(), ho);
+    std::copy(tot.oo.begin(), tot.oo.end(), oo);
+    return 0;
+  } catch (const std::exception& e) {
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
+}
+
 int oracle_cg_fixed(int n, int samples, const double* mean, const double* diag, const double* smp,
                     const double* g, double inv_w, double shift, double tol, int max_iter,
                     int diag_scale, double* x_out, double* z_apply) {

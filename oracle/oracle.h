@@ -50,6 +50,14 @@ int oracle_physcal_samples(const char* namelist, const char* zqp_opt, long long 
                            int64_t* proj_cnt, int64_t* counters, int64_t* draws,
                            uint32_t* next624, double* energies, char* err, int err_len);
 
+// Step 1 of an optimisation with W chains (seed + w): every walker's saved samples,
+// counters, draw counts, the O store [W][S][sr_size] and the reduced operands
+// (energy[5] = Wc, <E>, <E^2>, <Sz>, <Sz^2>; ho[sr_size]; oo[2*sr_size]).
+int oracle_opt_step1_walkers(const char* namelist, const char* initial_def, int walkers,
+                             long long seed, int64_t* ele_idx, int64_t* proj_cnt, int64_t* counters,
+                             int64_t* draws, double* energy, double* ho, double* oo, double* ostore,
+                             char* err, int err_len);
+
 // SR-CG on fixed operands (SampledSrOperator::solve_with_product): samples are
 // [samples][n]; returns the C status (iterations, or -(iter+1)). z_apply (optional)
 // receives S·g.

@@ -105,3 +105,20 @@ def cg_fixed(mean, diag, samples, g, inv_w, shift, tol, max_iter, diag_scale=Fal
 def hexline(line):
     import struct
     return np.array([struct.unpack(">d", bytes.fromhex(v))[0] for v in line.split()])
+
+
+def opt_step1_walkers(namelist, walkers, seed=-1, initial_def=""):
+    d = model_dims(namelist)
+    n, S, npj, size = 2 * d["ne"], d["nvmc_sample"], d["nproj"], 1 + d["npara"]
+    W = walkers
+    out = dict(ele_idx=np.zeros(W * S * n, np.int64), proj_cnt=np.zeros(W * S * npj, np.int64),
+               counter=np.zeros(W * 6, np.int64), draws=np.zeros(W, np.int64), energy=np.zeros(5),
+               ho=np.zeros(size), oo=np.zeros(2 * size), ostore=np.zeros(W * S * size))
+    err = err_buf()
+    rc = lib().oracle_opt_step1_walkers(namelist.encode(), initial_def.encode(), W, ctypes.c_longlong(seed),
+                                        *(ptr(out[k]) for k in ("ele_idx", "proj_cnt", "counter", "draws",
+                                                                "energy", "ho", "oo", "ostore")), err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    out["ostore"] = out["ostore"].reshape(W * S, size)
+    return d, out

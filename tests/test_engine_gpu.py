@@ -1,0 +1,152 @@
+"""Device engine parity: resident sampler, measurement and SR-CG against the native C
+golden vectors and the oracle, through the C ABI."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from mvmc_lib import mvmc, read_triples
+
+pytestmark = pytest.mark.gpu
+G = ol.GOLDEN
+
+
+def physcal_engine(precision=64):
+    d = os.path.join(G, "physcal_hubbard_chain_real")
+    m = mvmc()
+    eng = m.Engine(os.path.join(d, "inputs", "namelist.def"), walkers=1, precision=precision, seed=1)
+    p = read_triples(os.path.join(d, "zqp_opt.dat"), eng.dims["npara"])
+    nproj = eng.dims["nproj"]
+    f = p[nproj:]
+    p[nproj:] = f * (4.0 / np.abs(f).max())  # sync_modified_parameter: max |f| = 4
+    eng.set_parameters(p)
+    return d, eng
+
+
+def read_state(path):
+    out = {}
+    for line in open(path):
+        parts = line.split()
+        out[parts[0]] = [int(v) for v in parts[1:]]
+    return out
+
+
+def test_device_sampler_reproduces_native_c_trajectory():
+    """Every saved configuration, projection counter, C Counter[0..6] and the draw count
+    of two sample blocks of the native C sampler, from the device-resident sampler."""
+    d, eng = physcal_engine()
+    for b, idx in enumerate((7, 8)):
+        eng.sample()
+        got = eng.samples()
+        ref = read_state(os.path.join(d, "native-state", f"state_dump_{b:03d}.txt"))
+        assert got["ele_idx"].tolist() == ref["ele_idx"]
+        assert got["ele_cfg"].tolist() == ref["ele_cfg"]
+        assert got["ele_num"].tolist() == ref["ele_num"]
+        assert got["proj_cnt"].tolist() == ref["ele_proj_cnt"]
+        assert got["counter"].tolist() == ref["counter"][:6]
+        assert int(got["draws"][0]) == ref["draws"][0]
+        e, _, _ = eng.measure()
+        row = open(os.path.join(d, "expected", f"zvo_out_{idx:03d}.dat")).read().split()
+        assert abs(e[1] - float(row[0])) <= 1e-12 * abs(float(row[0]))
+        assert abs(e[2] - float(row[2])) <= 1e-12 * abs(float(row[2]))
+    assert eng.status() == 0
+
+
+def test_device_step1_sr_operands_match_native_c():
+    d = os.path.join(G, "sr_operands_hubbard")
+    eng = mvmc().Engine(os.path.join(d, "inputs", "namelist.def"), walkers=1, precision=64, seed=1)
+    eng.sample()
+    e, ho, oo = eng.measure()
+    ref = {}
+    for line in open(os.path.join(d, "hubbard-cg-store0.txt")):
+        if line.startswith("#"):
+            continue
+        name, rest = line.split(None, 1)
+        ref[name] = ol.hexline(rest)
+    assert abs(e[1] - ref["energy"][0]) <= 1e-12 * abs(ref["energy"][0])
+    for name, got in (("ho", ho), ("oo", oo)):
+        r = ref[name]
+        assert np.all(np.abs(got[: len(r)] - r) <= 1e-14 + 1e-13 * np.abs(r)), name
+    store = eng.o_store()
+    r = ref["o"]
+    assert np.all(np.abs(store[-1, : len(r)] - r) <= 1e-14 + 1e-13 * np.abs(r))
+
+
+@pytest.mark.parametrize("walkers", [1, 3, 8])
+def test_multiwalker_step1_matches_oracle(walkers):
+    """W chains seeded RndSeed + w: configurations exact, operands within 1e-12."""
+    nl = os.path.join(G, "sr_operands_hubbard", "inputs", "namelist.def")
+    dims, ref = ol.opt_step1_walkers(nl, walkers, seed=7)
+    eng = mvmc().Engine(nl, walkers=walkers, precision=64, seed=7)
+    eng.sample()
+    got = eng.samples()
+    assert got["ele_idx"].tolist() == ref["ele_idx"].tolist()
+    assert got["proj_cnt"].tolist() == ref["proj_cnt"].tolist()
+    assert got["counter"].tolist() == ref["counter"].tolist()
+    assert got["draws"].tolist() == ref["draws"].tolist()
+    e, ho, oo = eng.measure()
+    assert np.allclose(e, ref["energy"], rtol=1e-12, atol=1e-13)
+    assert np.allclose(ho, ref["ho"], rtol=1e-12, atol=1e-13)
+    assert np.allclose(oo, ref["oo"], rtol=1e-12, atol=1e-13)
+    assert np.allclose(eng.o_store(), ref["ostore"], rtol=1e-11, atol=1e-12)
+
+
+def read_cg_fixture(path):
+    lines = [l.rstrip("\n") for l in open(path) if not l.startswith("#")]
+    n, samples, _ = (int(v) for v in lines[0].split())
+    mean, diag, real = ol.hexline(lines[1]), ol.hexline(lines[2]), ol.hexline(lines[3])
+    g = ol.hexline(lines[5])
+    limits = []
+    for k in range(7, len(lines), 3):
+        head = lines[k].split(" ", 2)
+        limits.append((int(head[0]), int(head[1]), ol.hexline(head[2])))
+    return n, samples, mean, diag, real, g, limits
+
+
+@pytest.mark.parametrize("name,diag_scale", [("real.txt", False), ("real_diag_scale.txt", True)])
+def test_device_cg_recurrence_matches_native_c(name, diag_scale):
+    n, samples, mean, diag, real, g, limits = read_cg_fixture(os.path.join(G, "sr_cg", name))
+    m = mvmc()
+    for limit, status, x_ref in limits:
+        st, x = m.cg_solve(real, mean, diag, g, 1.0 / samples, 1e-5, 0.0, limit, diag_scale)
+        assert st == status, limit
+        if limit <= 5:
+            assert np.allclose(x, x_ref, rtol=1e-8, atol=1e-12 * np.abs(x_ref).max()), limit
+
+
+def test_device_cg_matches_oracle_on_random_operands():
+    rng = np.random.default_rng(5)
+    ns, na = 300, 40
+    smp = rng.normal(size=(ns, na))
+    mean = smp.mean(axis=0)
+    diag = (smp * smp).mean(axis=0) - mean * mean
+    g = rng.normal(size=na)
+    st, x = mvmc().cg_solve(smp, mean, diag, g, 1.0 / ns, 0.02, 1e-10, na)
+    ost, ox, _ = ol.cg_fixed(mean, diag, smp.ravel(), g, 1.0 / ns, 0.02, 1e-10, na)
+    assert st == ost
+    assert np.allclose(x, ox, rtol=1e-9, atol=1e-12)
+
+
+def read_out(path):
+    return np.array([[float(v) for v in line.split()] for line in open(path)])
+
+
+def test_full_optimisation_matches_oracle_zvo_out(tmp_path):
+    """Ten SR steps (sample → measure → SR-CG → sync) with 2 chains: zvo_out.dat energies
+    within 1e-8 of the oracle run, SRinfo rows and final parameters close."""
+    nl = os.path.join(G, "sr_operands_hubbard", "inputs", "namelist.def")
+    gdir, odir = tmp_path / "gpu", tmp_path / "oracle"
+    gdir.mkdir()
+    odir.mkdir()
+    ol.run_opt(nl, str(odir), walkers=2, nsteps=10, seed=3)
+    mvmc().run_opt(nl, str(gdir), nsteps=10, walkers=2, precision=64, seed=3)
+    a = read_out(gdir / "zvo_out.dat")
+    b = read_out(odir / "zvo_out.dat")
+    assert a.shape == b.shape == (10, 6)
+    assert np.all(np.abs(a[:, 0] - b[:, 0]) <= 1e-8 * np.abs(b[:, 0]))
+    va = read_out(gdir / "zvo_var.dat")
+    vb = read_out(odir / "zvo_var.dat")
+    assert np.allclose(va, vb, rtol=1e-7, atol=1e-9)
+    for name in ("zqp_opt.dat", "zvo_SRinfo.dat", "zqp_orbital_opt.dat"):
+        assert (gdir / name).exists() and (odir / name).exists()

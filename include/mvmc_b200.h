@@ -138,6 +138,12 @@ int mvmc_b200_status(mvmc_b200_ctx* ctx, unsigned* device_status);
 int mvmc_b200_run_opt(const char* namelist, const char* initial_def, const char* out_dir,
                       const mvmc_b200_options* opt, int nsteps);
 
+/* The context's CUDA stream (a cudaStream_t), for timing and ordering with caller work. */
+void* mvmc_b200_stream(mvmc_b200_ctx* ctx);
+
+/* Bytes the context copied host→device and device→host since creation (counters). */
+int mvmc_b200_transfer_bytes(const mvmc_b200_ctx* ctx, long long* h2d, long long* d2h);
+
 /* Last error message of the calling thread (empty when none). */
 const char* mvmc_b200_last_error(void);
 

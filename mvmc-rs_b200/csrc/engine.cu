@@ -109,6 +109,7 @@ struct mvmc_b200_ctx {
   int* d_map = nullptr;
   size_t map_cap = 0;
   std::vector<double> tot;  // host copy of the last reduction
+  long long h2d = 0, d2h = 0;  // bytes copied across the host boundary
   bool sampled = false, measured = false;
 
   template <typename T>
@@ -163,6 +164,8 @@ void upload_parameters(mvmc_b200_ctx* c) {
   check(cudaMemcpyAsync(c->d_gsite, gsite.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c->stream), "upload gsite");
   check(cudaMemcpyAsync(c->d_jpair, jpair.data(), sizeof(double) * jpair.size(), cudaMemcpyHostToDevice, c->stream),
         "upload jpair");
+  c->h2d += static_cast<long long>(sizeof(double)) *
+            (std::max<size_t>(1, m.slater.size()) + proj.size() + gsite.size() + jpair.size());
   const long long total = static_cast<long long>(m.nqp) * ns * ns;
   const int grid = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
   k_slater_table<<<std::max(1, grid), 256, 0, c->stream>>>(
@@ -178,7 +181,6 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
   mvmc::Model& m = c->m;
   m = mvmc::read_expert(namelist);
-  if (m.nsrcg == 0) m.nsrcg = 1;  // the device path solves SR by CG
   c->W = std::max(1, opt.walkers);
   c->S = opt.saved_per_walker > 0 ? opt.saved_per_walker : m.nvmc_sample;
   if (opt.precision != 64 && opt.precision != 32) throw std::runtime_error("precision must be 64 or 32");
@@ -339,6 +341,7 @@ int do_measure(mvmc_b200_ctx* c) {
   c->tot.assign(5 + 3 * c->dm.sr_size, 0.0);
   check(cudaMemcpyAsync(c->tot.data(), c->d_tot, sizeof(double) * c->tot.size(), cudaMemcpyDeviceToHost, c->stream),
         "download reduction");
+  c->d2h += static_cast<long long>(sizeof(double) * c->tot.size());
   check(cudaStreamSynchronize(c->stream), "measure");
   c->measured = true;
   return kOk;
@@ -349,6 +352,7 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   mvmc::Model& m = c->m;
   const int size = m.sr_size(), npara = m.npara();
   if (!c->measured) return MVMC_B200_ESTATE;
+  if (m.nsrcg == 0) throw std::runtime_error("direct SR (NSRCG 0) is not available on the device path; set NSRCG 1");
   if (m.rescale_smat) throw std::runtime_error("RescaleSmat is not supported by the device SR path");
   const double wc = c->tot[0];
   const double* ho = c->tot.data() + 5;
@@ -437,6 +441,8 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   check(cudaMemcpyAsync(x.data(), a.x, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
   check(cudaMemcpyAsync(scal.data(), c->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->stream), "download scal");
   check(cudaStreamSynchronize(c->stream), "sr-cg");
+  c->h2d += static_cast<long long>(sizeof(int) * na + sizeof(double) * 3 * na);
+  c->d2h += static_cast<long long>(sizeof(double) * (na + 8));
   long long status = static_cast<long long>(scal[1]);
   long long info = status;
   if (status < 0) {
@@ -602,6 +608,15 @@ extern "C" int mvmc_b200_get_local_energies(const mvmc_b200_ctx* c, double* e_lo
 extern "C" int mvmc_b200_sr_cg(mvmc_b200_ctx* c, double* sr_info) {
   if (!c) return MVMC_B200_EARG;
   return guarded([&]() { return do_sr_cg(c, sr_info); });
+}
+
+extern "C" void* mvmc_b200_stream(mvmc_b200_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+extern "C" int mvmc_b200_transfer_bytes(const mvmc_b200_ctx* c, long long* h2d, long long* d2h) {
+  if (!c || !h2d || !d2h) return MVMC_B200_EARG;
+  *h2d = c->h2d;
+  *d2h = c->d2h;
+  return MVMC_B200_OK;
 }
 
 extern "C" int mvmc_b200_status(mvmc_b200_ctx* c, unsigned* device_status) {

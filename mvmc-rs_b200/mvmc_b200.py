@@ -19,7 +19,7 @@ EXPORTS = [
     "mvmc_b200_get_parameters", "mvmc_b200_set_parameters", "mvmc_b200_sample",
     "mvmc_b200_get_samples", "mvmc_b200_measure", "mvmc_b200_get_o_store",
     "mvmc_b200_get_local_energies", "mvmc_b200_sr_cg", "mvmc_b200_status", "mvmc_b200_run_opt",
-    "mvmc_b200_last_error", "mvmc_b200_cg_solve",
+    "mvmc_b200_last_error", "mvmc_b200_cg_solve", "mvmc_b200_stream", "mvmc_b200_transfer_bytes",
 ]
 
 
@@ -36,6 +36,7 @@ def lib():
             raise RuntimeError(f"mvmc_b200: CUDA library not built ({LIB_PATH}); run make -C mvmc-rs_b200")
         _LIB = ctypes.CDLL(LIB_PATH)
         _LIB.mvmc_b200_last_error.restype = ctypes.c_char_p
+        _LIB.mvmc_b200_stream.restype = ctypes.c_void_p
     return _LIB
 
 
@@ -171,6 +172,15 @@ class Engine:
         info = np.zeros(9)
         rc = _check(lib().mvmc_b200_sr_cg(self.ctx, _ptr(info)), "sr_cg")
         return rc, info
+
+    def stream(self):
+        """The engine's cudaStream_t as an integer handle."""
+        return lib().mvmc_b200_stream(self.ctx)
+
+    def transfer_bytes(self):
+        h, d = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().mvmc_b200_transfer_bytes(self.ctx, ctypes.byref(h), ctypes.byref(d)), "transfer_bytes")
+        return h.value, d.value
 
     def status(self):
         s = ctypes.c_uint()

@@ -128,6 +128,24 @@ def test_device_cg_matches_oracle_on_random_operands():
     assert np.allclose(x, ox, rtol=1e-9, atol=1e-12)
 
 
+def cg_inputs(tmp_path, **overrides):
+    """Copy the Hubbard-chain inputs with the modpara overrides (NSRCG 1 selects SR-CG)."""
+    import shutil
+    src = os.path.join(G, "sr_operands_hubbard", "inputs")
+    dst = tmp_path / "inputs"
+    shutil.copytree(src, dst)
+    keys = {"NSRCG": "1", **{k: str(v) for k, v in overrides.items()}}
+    lines = open(dst / "modpara.def").read().splitlines()
+    for k, v in keys.items():
+        hit = [i for i, l in enumerate(lines) if l.split()[:1] == [k]]
+        if hit:
+            lines[hit[0]] = f"{k} {v}"
+        else:
+            lines.append(f"{k} {v}")
+    (dst / "modpara.def").write_text("\n".join(lines) + "\n")
+    return str(dst / "namelist.def")
+
+
 def read_out(path):
     return np.array([[float(v) for v in line.split()] for line in open(path)])
 
@@ -135,7 +153,7 @@ def read_out(path):
 def test_full_optimisation_matches_oracle_zvo_out(tmp_path):
     """Ten SR steps (sample → measure → SR-CG → sync) with 2 chains: zvo_out.dat energies
     within 1e-8 of the oracle run, SRinfo rows and final parameters close."""
-    nl = os.path.join(G, "sr_operands_hubbard", "inputs", "namelist.def")
+    nl = cg_inputs(tmp_path)
     gdir, odir = tmp_path / "gpu", tmp_path / "oracle"
     gdir.mkdir()
     odir.mkdir()

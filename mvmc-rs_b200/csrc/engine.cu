@@ -28,7 +28,7 @@ int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const d
 int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
                          double* oa, cudaStream_t stream);
 int launch_sr_cg(CgArgs a, cudaStream_t stream);
-int cg_grid_blocks();
+int cg_grid_blocks(long long ns, int na);
 
 // K0: SlaterElm[q][rs_i][rs_j] from the Slater parameters (update_slater_elm,
 // crates/mvmc-core/src/slater_update.rs:17-120).
@@ -402,7 +402,7 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
     c->d_map = c->alloc<int>(na);
     c->map_cap = na;
   }
-  const int blocks = cg_grid_blocks();
+  const int blocks = cg_grid_blocks(ns, na);
   const int ntile = (na + 255) / 256;
   const int nchunk = static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, blocks / ntile))));
   if (static_cast<size_t>(nchunk) * na > c->part_cap) {

@@ -24,8 +24,11 @@ namespace mvmcb {
 constexpr int kSampThreads = 256;
 
 struct SampLayout {
-  size_t sf, ctl, dctl, idx, cfg, num, cnt, cntn, cntm, pf, pfn, proj, qpw, vec, gj, ws, planes, total;
+  size_t sf, ctl, dctl, idx, cfg, num, cnt, cntn, cntm, pf, pfn, proj, qpw, jidx, vec, gj, ws, planes, total;
 };
+
+// The Jastrow index table is staged in shared memory for lattices up to this many sites.
+constexpr int kJidxSmemSites = 96;
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -46,6 +49,8 @@ __host__ __device__ inline SampLayout samp_layout(const DevModel& m, bool smem_p
   L.pfn = o; o = align16(o + sizeof(double) * m.nqp);
   L.proj = o; o = align16(o + sizeof(double) * (m.nproj + 1));
   L.qpw = o; o = align16(o + sizeof(double) * m.nqp);
+  L.jidx = o;
+  if (m.ns <= kJidxSmemSites) o = align16(o + sizeof(int) * static_cast<size_t>(m.ns) * m.ns);
   L.vec = o; o = align16(o + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n + sizeof(double) * 8 * m.nqp);
   L.gj = o; o = align16(o + gj_shared_bytes<double>(m.n));
   L.ws = o;
@@ -70,6 +75,7 @@ struct WalkerSmem {
   double* dctl;
   int *idx, *cfg, *num, *cnt, *cntn, *cntm;
   double *pf, *pfn, *proj, *qpw;
+  const int* jidx; // Jastrow index table (shared memory when small, else global)
   T* vec;          // [nqp][4][n]
   double* pscal;   // [nqp][8] per-plane scalars
   GJShared<double> gj;
@@ -114,8 +120,8 @@ __device__ void make_proj_cnt_serial(const DevModel& m, const int* num, int* cnt
 
 // update_proj_cnt by one warp; `num` accessor gives the occupation after the move.
 template <typename NumFn>
-__device__ void update_proj_cnt_warp(const DevModel& m, int ri, int rj, int* cnew, const int* cold,
-                                     NumFn num) {
+__device__ void update_proj_cnt_warp(const DevModel& m, const int* jtab, int ri, int rj, int* cnew,
+                                     const int* cold, NumFn num) {
   const int lane = threadIdx.x & 31;
   for (int k = lane; k < m.nproj; k += 32) cnew[k] = cold[k];
   __syncwarp();
@@ -128,7 +134,7 @@ __device__ void update_proj_cnt_warp(const DevModel& m, int ri, int rj, int* cne
   }
   if (m.n_jast > 0) {
     const int off = m.n_gutz;
-    auto jidx = [&](int a, int b) { return __ldg(m.jast_idx + min(a, b) * ns + max(a, b)); };
+    auto jidx = [&](int a, int b) { return jtab[min(a, b) * ns + max(a, b)]; };
     if (lane == 0) {
       const int ij = jidx(ri, rj);
       if (ij >= 0) atomicAdd(cnew + off + ij, (num(ri) + num(ri + ns)) - (num(rj) + num(rj + ns)) + 1);
@@ -209,10 +215,11 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
   __syncthreads();
   for (int k = tid; k < nq * n; k += nt) {
     const int q = k / n, j = k - q * n;
-    const T* P = s.planes + static_cast<size_t>(q) * n * n;
+    const T* P = s.planes + static_cast<size_t>(q) * n * n + j;
     const T* slt = vec + (q * 4 + 0) * n;
     T acc = T(0);
-    for (int i = 0; i < n; ++i) acc += -P[i * n + j] * slt[i];
+#pragma unroll 8
+    for (int i = 0; i < n; ++i) acc += -P[i * n] * slt[i];
     vec[(q * 4 + 1) * n + j] = acc;
   }
   __syncthreads();
@@ -224,17 +231,20 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
     if (j == 0) s.pf[q] *= -static_cast<double>(tmp);
   }
   __syncthreads();
-  const size_t total = static_cast<size_t>(nq) * n * n;
-  for (size_t k = tid; k < total; k += nt) {
-    const int q = static_cast<int>(k / (static_cast<size_t>(n) * n));
-    const int r = static_cast<int>(k - static_cast<size_t>(q) * n * n);
-    const int i = r / n, j = r - i * n;
+  // one warp per plane row: 32-bit indexing, row operands broadcast from shared memory
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  for (int row = warp; row < nq * n; row += nwarp) {
+    const int q = row / n, i = row - q * n;
     const T* v1 = vec + (q * 4 + 1) * n;
     const T* v2 = vec + (q * 4 + 2) * n;
-    T x = s.planes[k] + (v1[i] * v2[j] - v1[j] * v2[i]);
-    if (j == msa) x -= v2[i];
-    if (i == msa) x += v2[j];
-    s.planes[k] = x;
+    const T v1i = v1[i], v2i = v2[i];
+    T* P = s.planes + static_cast<size_t>(row) * n;
+    for (int j = lane; j < n; j += 32) {
+      T x = P[j] + (v1i * v2[j] - v1[j] * v2i);
+      if (j == msa) x -= v2i;
+      if (i == msa) x += v2[j];
+      P[j] = x;
+    }
   }
   __syncthreads();
 }
@@ -353,29 +363,29 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
     vec[(q * 4 + 1) * n + i] = idet * P[msb * n + i];
   }
   __syncthreads();
-  const size_t total = static_cast<size_t>(nq) * n * n;
-  for (size_t k = tid; k < total; k += nt) {
-    const int q = static_cast<int>(k / (static_cast<size_t>(n) * n));
-    const int r = static_cast<int>(k - static_cast<size_t>(q) * n * n);
-    const int i = r / n, j = r - i * n;
+  for (int row = warp; row < nq * n; row += nwarp) {
+    const int q = row / n, i = row - q * n;
     const double* o = sc + q * 8;
     const T a = o[0], b = o[1], c = o[2], d = o[3], e = o[4], f = o[5], idet = o[6], det = o[7];
+    const T edet = e * det, fidet = f * idet;
     const T* vs = vec + (q * 4 + 0) * n;
     const T* vt = vec + (q * 4 + 1) * n;
     const T* vp = vec + (q * 4 + 2) * n;
     const T* vq = vec + (q * 4 + 3) * n;
     const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
-    const T pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
-    T x = s.planes[k] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
-                         d * (pi * sj - pj * si) + e * det * (si * tj - sj * ti) +
-                         f * idet * (pi * qj - qi * pj));
-    if (j == msa) x += -c * ti - d * si - f * idet * qi;
-    if (j == msb) x += -a * ti - b * si + f * idet * pi;
-    if (i == msa) x += c * tj + d * sj + f * idet * qj;
-    if (i == msb) x += a * tj + b * sj - f * idet * pj;
-    if (i == msa && j == msb) x += f * idet;
-    if (i == msb && j == msa) x -= f * idet;
-    s.planes[k] = x;
+    T* P = s.planes + static_cast<size_t>(row) * n;
+    for (int j = lane; j < n; j += 32) {
+      const T pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
+      T x = P[j] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
+                    d * (pi * sj - pj * si) + edet * (si * tj - sj * ti) + fidet * (pi * qj - qi * pj));
+      if (j == msa) x += -c * ti - d * si - fidet * qi;
+      if (j == msb) x += -a * ti - b * si + fidet * pi;
+      if (i == msa) x += c * tj + d * sj + fidet * qj;
+      if (i == msb) x += a * tj + b * sj - fidet * pj;
+      if (i == msa && j == msb) x += fidet;
+      if (i == msb && j == msa) x -= fidet;
+      P[j] = x;
+    }
   }
   __syncthreads();
 }
@@ -441,6 +451,13 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
   s.pfn = reinterpret_cast<double*>(smem + L.pfn);
   s.proj = reinterpret_cast<double*>(smem + L.proj);
   s.qpw = reinterpret_cast<double*>(smem + L.qpw);
+  if (m.ns <= kJidxSmemSites) {
+    int* jt = reinterpret_cast<int*>(smem + L.jidx);
+    for (int k = threadIdx.x; k < m.ns * m.ns; k += blockDim.x) jt[k] = m.jast_idx[k];
+    s.jidx = jt;
+  } else {
+    s.jidx = m.jast_idx;
+  }
   s.vec = reinterpret_cast<T*>(smem + L.vec);
   s.pscal = reinterpret_cast<double*>(smem + L.vec + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n);
   s.gj = gj_carve<double>(smem + L.gj, m.n);
@@ -593,7 +610,7 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
       const int ri = cc[cRi], rj = cc[cRj], sp = cc[cS], msa = cc[cMsa];
       // --- projection counters (warp 0) and Pfaffian ratios (CTA) ---
       if (type == 0) {
-        if (tid < 32) update_proj_cnt_warp(m, ri, rj, s.cntn, s.cnt, [&](int k) { return s.num[k]; });
+        if (tid < 32) update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntn, s.cnt, [&](int k) { return s.num[k]; });
         ratio_hop_dev<T>(m, s, msa);
       } else {
         const int t = cc[cT];
@@ -601,8 +618,8 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
           // first move uses the occupation before the partner's move
           const int a = rj + t * ns, b = ri + t * ns;
           auto num_mid = [&](int k) { return k == a ? 1 : (k == b ? 0 : s.num[k]); };
-          update_proj_cnt_warp(m, ri, rj, s.cntm, s.cnt, num_mid);
-          update_proj_cnt_warp(m, rj, ri, s.cntn, s.cntm, [&](int k) { return s.num[k]; });
+          update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntm, s.cnt, num_mid);
+          update_proj_cnt_warp(m, s.jidx, rj, ri, s.cntn, s.cntm, [&](int k) { return s.num[k]; });
         }
         ratio_exchange_dev<T>(m, s, msa, cc[cMsb]);
       }

@@ -193,21 +193,24 @@ int launch_gather_active(const double* store, int sr_size, long long ns, const i
   return kOk;
 }
 
-int cg_grid_blocks() {
-  static int blocks = -1;
-  if (blocks < 0) {
+// Blocks of the cooperative solve: enough to stream the sample matrix (about 64K
+// elements per block), never more than are co-resident.
+int cg_grid_blocks(long long ns, int na) {
+  static int cap = -1;
+  if (cap < 0) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sr_cg, kCgThreads, 0);
-    blocks = sms * std::max(1, std::min(per, 4));
+    cap = sms * std::max(1, std::min(per, 4));
   }
-  return blocks;
+  const long long want = (ns * static_cast<long long>(na) + 65535) / 65536;
+  return static_cast<int>(std::max<long long>(1, std::min<long long>(cap, want)));
 }
 
 int launch_sr_cg(CgArgs a, cudaStream_t stream) {
   void* args[] = {&a};
-  MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_sr_cg), cg_grid_blocks(), kCgThreads,
+  MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_sr_cg), cg_grid_blocks(a.ns, a.na), kCgThreads,
                                          args, 0, stream));
   return kOk;
 }
@@ -230,7 +233,7 @@ extern "C" int mvmc_b200_cg_solve(const double* samples, long long ns, int na, c
                                   long long* status) {
   using namespace mvmcb;
   if (!samples || !mean || !diag || !g || !x || !status || na <= 0 || ns <= 0) return kErrArgument;
-  const int blocks = cg_grid_blocks();
+  const int blocks = cg_grid_blocks(ns, na);
   const int ntile = (na + 255) / 256;
   const int nchunk = static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, blocks / ntile))));
   Buf o, vec, y, part, red, scal;

@@ -134,7 +134,7 @@ def cg_inputs(tmp_path, **overrides):
     src = os.path.join(G, "sr_operands_hubbard", "inputs")
     dst = tmp_path / "inputs"
     shutil.copytree(src, dst)
-    keys = {"NSRCG": "1", **{k: str(v) for k, v in overrides.items()}}
+    keys = {"NSRCG": "1", "NSRCGAbortOnFail": "0", **{k: str(v) for k, v in overrides.items()}}
     lines = open(dst / "modpara.def").read().splitlines()
     for k, v in keys.items():
         hit = [i for i, l in enumerate(lines) if l.split()[:1] == [k]]
@@ -153,7 +153,8 @@ def read_out(path):
 def test_full_optimisation_matches_oracle_zvo_out(tmp_path):
     """Ten SR steps (sample → measure → SR-CG → sync) with 2 chains: zvo_out.dat energies
     within 1e-8 of the oracle run, SRinfo rows and final parameters close."""
-    nl = cg_inputs(tmp_path)
+    # a converging CG (tol 1e-8 reached in ~27 iterations): differences stay at rounding level
+    nl = cg_inputs(tmp_path, NSROptCGMaxIter=200, DSROptCGTol="1e-8")
     gdir, odir = tmp_path / "gpu", tmp_path / "oracle"
     gdir.mkdir()
     odir.mkdir()
@@ -168,3 +169,7 @@ def test_full_optimisation_matches_oracle_zvo_out(tmp_path):
     assert np.allclose(va, vb, rtol=1e-7, atol=1e-9)
     for name in ("zqp_opt.dat", "zvo_SRinfo.dat", "zqp_orbital_opt.dat"):
         assert (gdir / name).exists() and (odir / name).exists()
+    sa = [l.split() for l in open(gdir / "zvo_SRinfo.dat").read().splitlines()[1:]]
+    sb = [l.split() for l in open(odir / "zvo_SRinfo.dat").read().splitlines()[1:]]
+    assert [r[:4] for r in sa] == [r[:4] for r in sb]  # NPara, active size, cuts
+    assert all(int(r[-1]) >= 0 for r in sa)  # CG converged at every step

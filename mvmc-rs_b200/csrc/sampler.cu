@@ -21,7 +21,6 @@
 
 namespace mvmcb {
 
-constexpr int kSampThreads = 256;
 
 struct SampLayout {
   size_t sf, ctl, dctl, idx, cfg, num, cnt, cntn, cntm, pf, pfn, proj, qpw, jidx, vec, gj, ws, planes, total;
@@ -66,7 +65,16 @@ enum Ctl {
   cSkip = 0, cType, cMi, cRi, cRj, cS, cMj, cT, cMsa, cMsb, cAccept, cRefresh, cInfo, cNacc,
   cBurn, cAttempt, cStop
 };
-enum DCtl { dLogIp = 0, dLogIpNew = 1 };
+enum DCtl { dLogIp = 0, dLogIpNew = 1, dDproj = 2 };
+
+// Δ ln P = Σ_k α_k (c'_k − c_k) by one warp (log_proj_ratio, projection.rs:403).
+__device__ __forceinline__ double log_proj_ratio_warp(int nproj, const double* proj, const int* cnew,
+                                                      const int* cold) {
+  const int lane = threadIdx.x & 31;
+  double z = 0.0;
+  for (int k = lane; k < nproj; k += 32) z += proj[k] * static_cast<double>(cnew[k] - cold[k]);
+  return warp_sum(z);
+}
 
 template <typename T>
 struct WalkerSmem {
@@ -202,10 +210,17 @@ __device__ void ratio_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa
   }
 }
 
-// ---- rank-2 update of an accepted hop (update_one_real) -----------------------------------
-template <typename T>
+// Lane-owned columns: lane l of every warp owns columns j = l + 32c (c < JPL) of every
+// plane row it touches, so column vectors of the rank-2/rank-4 updates sit in registers
+// and only the row scalars are broadcast from shared memory.
+
+// ---- rank-2 update of an accepted hop (update_one_real, updates.rs:1154-1215) --------------
+//   vec1 = −InvMᵀ·slt,  pf ← −pf·vec1[msa],  vec2 = InvM[msa]·(−1/vec1[msa]),
+//   InvM += vec1⊗vec2 − vec2⊗vec1, then column msa −= vec2 and row msa += vec2.
+template <typename T, int JPL>
 __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa) {
   const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   const int rsa = rs_of(m, s.idx, msa);
   T* vec = s.vec;  // [q][0]=slt, [1]=vec1, [2]=vec2
   for (int k = tid; k < nq * n; k += nt) {
@@ -213,7 +228,7 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
     vec[(q * 4 + 0) * n + i] = slater_at<T>(m, q, rsa, rs_of(m, s.idx, i));
   }
   __syncthreads();
-  for (int k = tid; k < nq * n; k += nt) {
+  for (int k = tid; k < nq * n; k += nt) {  // column form: one thread per (plane, column)
     const int q = k / n, j = k - q * n;
     const T* P = s.planes + static_cast<size_t>(q) * n * n + j;
     const T* slt = vec + (q * 4 + 0) * n;
@@ -231,31 +246,52 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
     if (j == 0) s.pf[q] *= -static_cast<double>(tmp);
   }
   __syncthreads();
-  // one warp per plane row: 32-bit indexing, row operands broadcast from shared memory
-  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
-  for (int row = warp; row < nq * n; row += nwarp) {
-    const int q = row / n, i = row - q * n;
+  const int cmsa = msa >> 5, lmsa = msa & 31;
+  for (int q = 0; q < nq; ++q) {
     const T* v1 = vec + (q * 4 + 1) * n;
     const T* v2 = vec + (q * 4 + 2) * n;
-    const T v1i = v1[i], v2i = v2[i];
-    T* P = s.planes + static_cast<size_t>(row) * n;
-    for (int j = lane; j < n; j += 32) {
-      T x = P[j] + (v1i * v2[j] - v1[j] * v2i);
-      if (j == msa) x -= v2i;
-      if (i == msa) x += v2[j];
-      P[j] = x;
+    T v1c[JPL], v2c[JPL];
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      v1c[c] = j < n ? v1[j] : T(0);
+      v2c[c] = j < n ? v2[j] : T(0);
+    }
+    T* P = s.planes + static_cast<size_t>(q) * n * n;
+    for (int i = warp; i < n; i += nwarp) {
+      const T v1i = v1[i], v2i = v2[i];
+      T* Pi = P + static_cast<size_t>(i) * n;
+      if (i != msa) {
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j < n) Pi[j] = Pi[j] + (v1i * v2c[c] - v1c[c] * v2i);
+        }
+        if (lane == lmsa) Pi[msa] -= v2i;  // the thread that owns column msa of this row
+      } else {
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j < n) {
+            T x = Pi[j] + (v1i * v2c[c] - v1c[c] * v2i);
+            if (c == cmsa && lane == lmsa) x -= v2i;
+            Pi[j] = x + v2c[c];
+          }
+        }
+      }
     }
   }
   __syncthreads();
 }
 
 // ---- exchange ratio (two_ratio_real, updates.rs:1539-1622) --------------------------------
+//   ratio = InvM_ab·vb_a + InvM_ab·(vbᵀ·InvM·va) + p_a q_b − p_b q_a
 template <typename T>
 __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, int msb) {
   const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   const int rsa = rs_of(m, s.idx, msa), rsb = rs_of(m, s.idx, msb);
-  T* vec = s.vec;  // [0]=va, [1]=vb, [2]=inv·va
+  T* vec = s.vec;  // [0]=va, [1]=vb, [2]=InvM·va
   for (int k = tid; k < nq * n; k += nt) {
     const int q = k / n, i = k - q * n;
     const int ri = rs_of(m, s.idx, i);
@@ -263,14 +299,15 @@ __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, in
     vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
   }
   __syncthreads();
-  for (int row = warp; row < nq * n; row += nwarp) {
-    const int q = row / n, i = row - q * n;
-    const T* P = s.planes + (static_cast<size_t>(q) * n + i) * n;
+  // (InvM·va)[i] = −Σ_j InvM[j][i]·va[j] (skew symmetry), one thread per (plane, i)
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, i = k - q * n;
+    const T* P = s.planes + static_cast<size_t>(q) * n * n + i;
     const T* va = vec + (q * 4 + 0) * n;
     T t = T(0);
-    for (int j = lane; j < n; j += 32) t += P[j] * va[j];
-    t = warp_sum(t);
-    if (lane == 0) vec[(q * 4 + 2) * n + i] = t;
+#pragma unroll 8
+    for (int j = 0; j < n; ++j) t += P[j * n] * va[j];
+    vec[(q * 4 + 2) * n + i] = -t;
   }
   __syncthreads();
   for (int q = warp; q < nq; q += nwarp) {
@@ -300,7 +337,7 @@ __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, in
 }
 
 // ---- rank-4 update of an accepted exchange (update_two_real, updates.rs:1429-1505) --------
-template <typename T>
+template <typename T, int JPL>
 __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, int msb,
                                     int rsa_old, int rsb_old) {
   const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
@@ -314,22 +351,21 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
     vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
   }
   __syncthreads();
-  for (int row = warp; row < nq * n; row += nwarp) {
-    const int q = row / n, i = row - q * n;
-    const T* P = s.planes + (static_cast<size_t>(q) * n + i) * n;
+  // vp = InvM·vs, vq = InvM·vt in column form (skew symmetry)
+  for (int k = tid; k < nq * n; k += nt) {
+    const int q = k / n, i = k - q * n;
+    const T* P = s.planes + static_cast<size_t>(q) * n * n + i;
     const T* vs = vec + (q * 4 + 0) * n;
     const T* vt = vec + (q * 4 + 1) * n;
     T p = T(0), r = T(0);
-    for (int j = lane; j < n; j += 32) {
-      p += P[j] * vs[j];
-      r += P[j] * vt[j];
+#pragma unroll 8
+    for (int j = 0; j < n; ++j) {
+      const T x = P[j * n];
+      p += x * vs[j];
+      r += x * vt[j];
     }
-    p = warp_sum(p);
-    r = warp_sum(r);
-    if (lane == 0) {
-      vec[(q * 4 + 2) * n + i] = p;
-      vec[(q * 4 + 3) * n + i] = r;
-    }
+    vec[(q * 4 + 2) * n + i] = -p;
+    vec[(q * 4 + 3) * n + i] = -r;
   }
   __syncthreads();
   double* sc = s.pscal;  // per plane: a b c d e f idet det
@@ -363,8 +399,7 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
     vec[(q * 4 + 1) * n + i] = idet * P[msb * n + i];
   }
   __syncthreads();
-  for (int row = warp; row < nq * n; row += nwarp) {
-    const int q = row / n, i = row - q * n;
+  for (int q = 0; q < nq; ++q) {
     const double* o = sc + q * 8;
     const T a = o[0], b = o[1], c = o[2], d = o[3], e = o[4], f = o[5], idet = o[6], det = o[7];
     const T edet = e * det, fidet = f * idet;
@@ -372,19 +407,37 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
     const T* vt = vec + (q * 4 + 1) * n;
     const T* vp = vec + (q * 4 + 2) * n;
     const T* vq = vec + (q * 4 + 3) * n;
-    const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
-    T* P = s.planes + static_cast<size_t>(row) * n;
-    for (int j = lane; j < n; j += 32) {
-      const T pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
-      T x = P[j] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
-                    d * (pi * sj - pj * si) + edet * (si * tj - sj * ti) + fidet * (pi * qj - qi * pj));
-      if (j == msa) x += -c * ti - d * si - fidet * qi;
-      if (j == msb) x += -a * ti - b * si + fidet * pi;
-      if (i == msa) x += c * tj + d * sj + fidet * qj;
-      if (i == msb) x += a * tj + b * sj - fidet * pj;
-      if (i == msa && j == msb) x += fidet;
-      if (i == msb && j == msa) x -= fidet;
-      P[j] = x;
+    T pc[JPL], qc[JPL], sc_[JPL], tc[JPL];
+#pragma unroll
+    for (int c2 = 0; c2 < JPL; ++c2) {
+      const int j = lane + 32 * c2;
+      pc[c2] = j < n ? vp[j] : T(0);
+      qc[c2] = j < n ? vq[j] : T(0);
+      sc_[c2] = j < n ? vs[j] : T(0);
+      tc[c2] = j < n ? vt[j] : T(0);
+    }
+    T* P = s.planes + static_cast<size_t>(q) * n * n;
+    for (int i = warp; i < n; i += nwarp) {
+      const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
+      T* Pi = P + static_cast<size_t>(i) * n;
+      const bool row_fix = (i == msa) || (i == msb);
+#pragma unroll
+      for (int c2 = 0; c2 < JPL; ++c2) {
+        const int j = lane + 32 * c2;
+        if (j >= n) continue;
+        const T pj = pc[c2], qj = qc[c2], sj = sc_[c2], tj = tc[c2];
+        T x = Pi[j] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
+                       d * (pi * sj - pj * si) + edet * (si * tj - sj * ti) + fidet * (pi * qj - qi * pj));
+        if (j == msa) x += -c * ti - d * si - fidet * qi;
+        if (j == msb) x += -a * ti - b * si + fidet * pi;
+        if (row_fix) {
+          if (i == msa) x += c * tj + d * sj + fidet * qj;
+          if (i == msb) x += a * tj + b * sj - fidet * pj;
+          if (i == msa && j == msb) x += fidet;
+          if (i == msb && j == msa) x -= fidet;
+        }
+        Pi[j] = x;
+      }
     }
   }
   __syncthreads();
@@ -431,8 +484,8 @@ __device__ void make_initial_sample_dev(const DevModel& m, SfmtRef& rng, int* id
   make_proj_cnt_serial(m, num, cnt);
 }
 
-template <typename T, bool kSmemPlanes, bool kSmemWs>
-__global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers w) {
+template <typename T, int JPL, int NT, bool kSmemPlanes, bool kSmemWs>
+__global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int wk = blockIdx.x;
   const int tid = threadIdx.x;
@@ -610,7 +663,11 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
       const int ri = cc[cRi], rj = cc[cRj], sp = cc[cS], msa = cc[cMsa];
       // --- projection counters (warp 0) and Pfaffian ratios (CTA) ---
       if (type == 0) {
-        if (tid < 32) update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntn, s.cnt, [&](int k) { return s.num[k]; });
+        if (tid < 32) {
+          update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntn, s.cnt, [&](int k) { return s.num[k]; });
+          const double z = log_proj_ratio_warp(m.nproj, s.proj, s.cntn, s.cnt);
+          if (tid == 0) s.dctl[dDproj] = z;
+        }
         ratio_hop_dev<T>(m, s, msa);
       } else {
         const int t = cc[cT];
@@ -620,6 +677,8 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
           auto num_mid = [&](int k) { return k == a ? 1 : (k == b ? 0 : s.num[k]); };
           update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntm, s.cnt, num_mid);
           update_proj_cnt_warp(m, s.jidx, rj, ri, s.cntn, s.cntm, [&](int k) { return s.num[k]; });
+          const double z = log_proj_ratio_warp(m.nproj, s.proj, s.cntn, s.cnt);
+          if (tid == 0) s.dctl[dDproj] = z;
         }
         ratio_exchange_dev<T>(m, s, msa, cc[cMsb]);
       }
@@ -629,8 +688,7 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
         double ip = 0.0;
         for (int q = 0; q < m.nqp; ++q) ip += s.qpw[q] * s.pfn[q];
         const double lip_new = log(fabs(ip));
-        double dproj = 0.0;
-        for (int k = 0; k < m.nproj; ++k) dproj += s.proj[k] * static_cast<double>(s.cntn[k] - s.cnt[k]);
+        const double dproj = s.dctl[dDproj];
         double wgt = exp(2.0 * ((dproj + 0.0 + lip_new) - s.dctl[dLogIp]));
         if (!isfinite(wgt)) wgt = -1.0;
         const double u = rng.real2();
@@ -661,9 +719,9 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
       __syncthreads();
       if (cc[cAccept]) {
         if (type == 0) {
-          update_hop_dev<T>(m, s, msa);
+          update_hop_dev<T, JPL>(m, s, msa);
         } else {
-          update_exchange_dev<T>(m, s, msa, cc[cMsb], ri + sp * ns, rj + cc[cT] * ns);
+          update_exchange_dev<T, JPL>(m, s, msa, cc[cMsb], ri + sp * ns, rj + cc[cT] * ns);
         }
       }
       if (cc[cRefresh]) {
@@ -704,12 +762,12 @@ __global__ void __launch_bounds__(kSampThreads) k_sample(DevModel m, DevWalkers 
 // ---- host launch ---------------------------------------------------------------------------
 int smem_limit_bytes();
 
-template <typename T, bool kSmemPlanes, bool kSmemWs>
+template <typename T, int JPL, int NT, bool kSmemPlanes, bool kSmemWs>
 int launch_sample_t(const DevModel& m, const DevWalkers& w, cudaStream_t stream) {
   const size_t smem = samp_layout<T>(m, kSmemPlanes, kSmemWs).total;
-  MVMCB_CUDA(cudaFuncSetAttribute(k_sample<T, kSmemPlanes, kSmemWs>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  k_sample<T, kSmemPlanes, kSmemWs><<<w.W, kSampThreads, smem, stream>>>(m, w);
+  auto kernel = k_sample<T, JPL, NT, kSmemPlanes, kSmemWs>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  kernel<<<w.W, NT, smem, stream>>>(m, w);
   MVMCB_CUDA(cudaGetLastError());
   return kOk;
 }
@@ -722,20 +780,33 @@ bool sample_planes_in_smem(const DevModel& m, int precision, int limit) {
   return samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit);
 }
 
+template <int JPL>
+int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int limit, cudaStream_t stream) {
+  // Resident (shared-memory) planes run one walker per SM with 16 warps; planes in global
+  // memory run several walkers per SM with 8 warps each.
+  if (precision == 32) {
+    if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit))
+      return launch_sample_t<float, JPL, 512, true, true>(m, w, stream);
+    if (samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit))
+      return launch_sample_t<float, JPL, 512, true, false>(m, w, stream);
+    return launch_sample_t<float, JPL, 256, false, false>(m, w, stream);
+  }
+  if (samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit))
+    return launch_sample_t<double, JPL, 512, true, false>(m, w, stream);
+  return launch_sample_t<double, JPL, 256, false, false>(m, w, stream);
+}
+
 int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStream_t stream) {
   int dev = 0, limit = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (precision == 32) {
-    if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit))
-      return launch_sample_t<float, true, true>(m, w, stream);
-    if (samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit))
-      return launch_sample_t<float, true, false>(m, w, stream);
-    return launch_sample_t<float, false, false>(m, w, stream);
-  }
-  if (samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit))
-    return launch_sample_t<double, true, false>(m, w, stream);
-  return launch_sample_t<double, false, false>(m, w, stream);
+  const int n = m.n;
+  if (n <= 32) return launch_sample_jpl<1>(m, w, precision, limit, stream);
+  if (n <= 64) return launch_sample_jpl<2>(m, w, precision, limit, stream);
+  if (n <= 128) return launch_sample_jpl<4>(m, w, precision, limit, stream);
+  if (n <= 224) return launch_sample_jpl<7>(m, w, precision, limit, stream);
+  if (n <= 256) return launch_sample_jpl<8>(m, w, precision, limit, stream);
+  return kErrArgument;
 }
 
 }  // namespace mvmcb

@@ -242,6 +242,9 @@ def main():
             "e2e": {"value": sweeps_total / (t_wall_ms / 1e3), "unit": "sweeps/s",
                     "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps},
             "gpu_launches": 8 * args.steps,
+            "residency": os.environ.get("MVMC_B200_RESIDENCY", "auto"),
+            "phase_cycles_per_walker": ({k: v / W for k, v in eng.sampler_timers().items()}
+                                        if os.environ.get("MVMC_B200_TIMERS") == "1" else None),
             "clocks": clocks,
         }
         print(json.dumps(out), flush=True)

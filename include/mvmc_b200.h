@@ -138,6 +138,12 @@ int mvmc_b200_status(mvmc_b200_ctx* ctx, unsigned* device_status);
 int mvmc_b200_run_opt(const char* namelist, const char* initial_def, const char* out_dir,
                       const mvmc_b200_options* opt, int nsteps);
 
+/* Sampler phase timers (the device analogue of the C timers of the sampler substeps):
+ * cycles[8] = {candidate, ratio, metropolis, update, refresh, total, -, -} summed over walkers
+ * for the last mvmc_b200_sample, measured by each walker's control thread. Zero unless the
+ * environment variable MVMC_B200_TIMERS=1 was set when the context was created. */
+int mvmc_b200_sampler_timers(const mvmc_b200_ctx* ctx, double* cycles);
+
 /* The context's CUDA stream (a cudaStream_t), for timing and ordering with caller work. */
 void* mvmc_b200_stream(mvmc_b200_ctx* ctx);
 

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -291,6 +292,13 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   dw.status = c->alloc<unsigned>(1);
   check(cudaMemset(dw.status, 0, sizeof(unsigned)), "memset status");
   dw.refresh_sweeps = opt.refresh_sweeps;
+  dw.timers = nullptr;
+  if (const char* t = std::getenv("MVMC_B200_TIMERS")) {
+    if (std::strcmp(t, "1") == 0) {
+      dw.timers = c->alloc<unsigned long long>(static_cast<size_t>(W) * kPhCount);
+      check(cudaMemset(dw.timers, 0, sizeof(unsigned long long) * W * kPhCount), "memset timers");
+    }
+  }
   int dev = 0, limit = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -608,6 +616,19 @@ extern "C" int mvmc_b200_get_local_energies(const mvmc_b200_ctx* c, double* e_lo
 extern "C" int mvmc_b200_sr_cg(mvmc_b200_ctx* c, double* sr_info) {
   if (!c) return MVMC_B200_EARG;
   return guarded([&]() { return do_sr_cg(c, sr_info); });
+}
+
+extern "C" int mvmc_b200_sampler_timers(const mvmc_b200_ctx* c, double* cycles) {
+  if (!c || !cycles) return MVMC_B200_EARG;
+  std::fill(cycles, cycles + kPhCount, 0.0);
+  if (!c->dw.timers) return MVMC_B200_OK;
+  return guarded([&]() {
+    std::vector<unsigned long long> t(static_cast<size_t>(c->W) * kPhCount);
+    check(cudaMemcpy(t.data(), c->dw.timers, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost), "timers");
+    for (int w = 0; w < c->W; ++w)
+      for (int k = 0; k < kPhCount; ++k) cycles[k] += static_cast<double>(t[static_cast<size_t>(w) * kPhCount + k]);
+    return MVMC_B200_OK;
+  });
 }
 
 extern "C" void* mvmc_b200_stream(mvmc_b200_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }

@@ -59,7 +59,12 @@ struct DevWalkers {
   int* s_cnt;                 // [W*saved*nproj]
   unsigned* status;           // [1] sticky
   int refresh_sweeps;         // mixed path: extra FP64 refresh cadence in sweeps (0 = off)
+  unsigned long long* timers; // [W*8] clock cycles per sampler phase, or null (off)
 };
+
+// Sampler phases timed by thread 0 of each walker (cycles, barrier waits included):
+// candidate, ratio, metropolis, update, refresh, total.
+enum SamplerPhase { kPhCandidate = 0, kPhRatio, kPhMetropolis, kPhUpdate, kPhRefresh, kPhTotal, kPhCount = 8 };
 
 // Arguments of the cooperative SR-CG solve.
 struct CgArgs {

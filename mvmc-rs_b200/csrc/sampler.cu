@@ -14,6 +14,9 @@
 // global slice (L2-resident working set).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+#include <cstring>
+
 #include "common.cuh"
 #include "engine.cuh"
 #include "pfinv.cuh"
@@ -577,6 +580,17 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
   long long since_refresh = 0;
 
   long long proposal = 0;
+  unsigned long long ph[kPhCount] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const bool timing = w.timers != nullptr && tid == 0;
+  unsigned long long t_last = timing ? clock64() : 0ULL;
+  const unsigned long long t_begin = t_last;
+  auto lap = [&](int phase) {
+    if (timing) {
+      const unsigned long long t = clock64();
+      ph[phase] += t - t_last;
+      t_last = t;
+    }
+  };
   for (int out = 0; out < n_out; ++out) {
     for (int step = 0; step < n_in; ++step, ++proposal) {
       // Candidate slots alternate between two banks: a skipped proposal has no later
@@ -658,6 +672,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
         cc[cSkip] = skip;
       }
       __syncthreads();
+      lap(kPhCandidate);
       if (cc[cSkip]) continue;
       const int type = cc[cType];
       const int ri = cc[cRi], rj = cc[cRj], sp = cc[cS], msa = cc[cMsa];
@@ -683,6 +698,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
         ratio_exchange_dev<T>(m, s, msa, cc[cMsb]);
       }
       __syncthreads();
+      lap(kPhRatio);
       // --- Metropolis (thread 0) ---
       if (tid == 0) {
         double ip = 0.0;
@@ -717,6 +733,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
         cc[cRefresh] = refresh;
       }
       __syncthreads();
+      lap(kPhMetropolis);
       if (cc[cAccept]) {
         if (type == 0) {
           update_hop_dev<T, JPL>(m, s, msa);
@@ -724,11 +741,13 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
           update_exchange_dev<T, JPL>(m, s, msa, cc[cMsb], ri + sp * ns, rj + cc[cT] * ns);
         }
       }
+      lap(kPhUpdate);
       if (cc[cRefresh]) {
         const int info = calc_m_all_dev<T>(m, s, w.status);
         if (tid == 0 && info == 0 && cc[cRefresh] == 1) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
         if (tid == 0 && info == 0 && cc[cRefresh] == 2) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
         __syncthreads();
+        lap(kPhRefresh);
       }
     }
     if (out + S >= n_out) {
@@ -756,6 +775,10 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
     w.draws[wk] = sf_draws;
     w.burn[wk] = 1;
     for (int k = 0; k < 6; ++k) w.counter[static_cast<size_t>(wk) * 6 + k] = counter[k];
+    if (timing) {
+      ph[kPhTotal] = clock64() - t_begin;
+      for (int k = 0; k < kPhCount; ++k) w.timers[static_cast<size_t>(wk) * kPhCount + k] = ph[k];
+    }
   }
 }
 
@@ -774,16 +797,36 @@ int launch_sample_t(const DevModel& m, const DevWalkers& w, cudaStream_t stream)
 
 // Shared-memory residency: planes (and for FP32 the FP64 refresh workspace) in shared
 // memory when they fit the per-block opt-in limit.
+int residency_policy();
 bool sample_planes_in_smem(const DevModel& m, int precision, int limit) {
+  if (residency_policy() == 1) return false;
   if (precision == 32) return samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit) ||
                               samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit);
   return samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit);
+}
+
+// Plane residency: "shared" keeps a walker's planes in shared memory (one walker per SM
+// when they are large), "global" keeps them in the walker's L2-resident slice so several
+// walkers share an SM; "auto" (default) prefers shared memory. MVMC_B200_RESIDENCY selects.
+int residency_policy() {
+  static int policy = -1;
+  if (policy < 0) {
+    const char* v = std::getenv("MVMC_B200_RESIDENCY");
+    policy = 0;
+    if (v && std::strcmp(v, "global") == 0) policy = 1;
+    if (v && std::strcmp(v, "shared") == 0) policy = 2;
+  }
+  return policy;
 }
 
 template <int JPL>
 int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int limit, cudaStream_t stream) {
   // Resident (shared-memory) planes run one walker per SM with 16 warps; planes in global
   // memory run several walkers per SM with 8 warps each.
+  if (residency_policy() == 1) {
+    if (precision == 32) return launch_sample_t<float, JPL, 256, false, false>(m, w, stream);
+    return launch_sample_t<double, JPL, 256, false, false>(m, w, stream);
+  }
   if (precision == 32) {
     if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit))
       return launch_sample_t<float, JPL, 512, true, true>(m, w, stream);

@@ -20,6 +20,7 @@ EXPORTS = [
     "mvmc_b200_get_samples", "mvmc_b200_measure", "mvmc_b200_get_o_store",
     "mvmc_b200_get_local_energies", "mvmc_b200_sr_cg", "mvmc_b200_status", "mvmc_b200_run_opt",
     "mvmc_b200_last_error", "mvmc_b200_cg_solve", "mvmc_b200_stream", "mvmc_b200_transfer_bytes",
+    "mvmc_b200_sampler_timers",
 ]
 
 
@@ -181,6 +182,12 @@ class Engine:
         h, d = ctypes.c_longlong(), ctypes.c_longlong()
         _check(lib().mvmc_b200_transfer_bytes(self.ctx, ctypes.byref(h), ctypes.byref(d)), "transfer_bytes")
         return h.value, d.value
+
+    def sampler_timers(self):
+        c = np.zeros(8)
+        _check(lib().mvmc_b200_sampler_timers(self.ctx, _ptr(c)), "sampler_timers")
+        keys = ["candidate", "ratio", "metropolis", "update", "refresh", "total"]
+        return dict(zip(keys, c[:6].tolist()))
 
     def status(self):
         s = ctypes.c_uint()

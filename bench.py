@@ -109,6 +109,8 @@ def main():
     ap.add_argument("--config", default="square8")
     ap.add_argument("--precision", type=int, default=64)
     ap.add_argument("--walkers", type=int, default=0)
+    ap.add_argument("--refresh", type=int, default=32,
+                    help="mixed path: FP64 refresh every this many sweeps (0: the C accept-window rule)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     ws, rank, local = dist_env()
@@ -154,7 +156,7 @@ def main():
                                 timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     eng = mb.Engine(namelist, initial_def, walkers=W, precision=args.precision, seed=12345 + rank * W,
-                    device=local)
+                    device=local, refresh_sweeps=args.refresh if args.precision == 32 else 0)
     stream = torch.cuda.ExternalStream(eng.stream())
     info = {}
 
@@ -231,6 +233,7 @@ def main():
             "config": {"workload": args.config, "walkers_per_gpu": W, "nsite": ns, "n": n, "nqp": nqp,
                        "npara": dims["npara"], "sweeps_per_walker_step": sweeps_per_walker_step,
                        "precision": args.precision, "parallelism": f"replicas{ws}",
+                       "refresh_sweeps": args.refresh if args.precision == 32 else None,
                        "l2": "inputs larger than L2 between steps (walker planes + O matrix)"},
             "sr_step_ms": ms / args.steps, "sample_ms": samp_avg_ms, "energy": info.get("energy"),
             "acceptance": p_acc,

@@ -311,7 +311,8 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
     if (opt.precision == 64) dw.inv = c->alloc<double>(static_cast<size_t>(W) * nqp * nn);
     else dw.inv = c->alloc<float>(static_cast<size_t>(W) * nqp * nn);
   }
-  if (opt.precision == 32) dw.ws64 = c->alloc<double>(static_cast<size_t>(W) * nn);
+  // FP64 sweep buffers of walkers whose buffers are not in shared memory (two per walker)
+  dw.ws64 = c->alloc<double>(static_cast<size_t>(W) * 2 * nn);
   // measurement
   const size_t rows = static_cast<size_t>(W) * S;
   c->d_ostore = c->alloc<double>(rows * dm.sr_size);
@@ -320,7 +321,7 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   c->d_wsum = c->alloc<double>(static_cast<size_t>(W) * (5 + 3 * dm.sr_size));
   c->d_tot = c->alloc<double>(5 + 3 * dm.sr_size);
   c->gws_blocks = std::min<int>(static_cast<int>(rows), sms * 8);
-  c->d_gws = c->alloc<double>(static_cast<size_t>(c->gws_blocks) * nn);
+  c->d_gws = c->alloc<double>(static_cast<size_t>(c->gws_blocks) * 2 * nn);
   c->d_red = c->alloc<double>(4096);
   c->d_scal = c->alloc<double>(8);
   upload_parameters(c);

@@ -15,6 +15,8 @@
 // bitwise repeatable up to the O_k scatter (shared-memory atomics).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "engine.cuh"
 #include "pfinv.cuh"
@@ -43,14 +45,15 @@ __host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_p
   L.g1 = o; o = a16(o + sizeof(double) * (m.nterm + 1));
   L.oacc = o; o = a16(o + sizeof(double) * (m.norb + 1));
   L.cj = o; o = a16(o + sizeof(double) * m.ns);
-  L.gj = o; o = a16(o + gj_shared_bytes<double>(m.n));
+  L.gj = o;
   L.plane = o;
-  if (smem_plane) o = a16(o + sizeof(double) * static_cast<size_t>(m.n) * m.n);
+  // the plane and its ping-pong partner
+  if (smem_plane) o = a16(o + 2 * sizeof(double) * static_cast<size_t>(m.n) * m.n);
   L.total = o;
   return L;
 }
 
-template <bool kSmemPlane>
+template <int JPL, bool kSmemPlane>
 __global__ void __launch_bounds__(kMeasThreads)
     k_measure(DevModel m, const int* __restrict__ s_idx, const int* __restrict__ s_cfg,
               const int* __restrict__ s_num, const int* __restrict__ s_cnt, int nsamples,
@@ -69,11 +72,11 @@ __global__ void __launch_bounds__(kMeasThreads)
   double* g1 = reinterpret_cast<double*>(smem + L.g1);
   double* oacc = reinterpret_cast<double*>(smem + L.oacc);
   double* cj = reinterpret_cast<double*>(smem + L.cj);
-  GJShared<double> gj = gj_carve<double>(smem + L.gj, m.n);
   const int n = m.n, ns = m.ns, ne = m.ne, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   const size_t nn = static_cast<size_t>(n) * n;
-  double* A = kSmemPlane ? reinterpret_cast<double*>(smem + L.plane) : gws + static_cast<size_t>(blockIdx.x) * nn;
+  double* A = kSmemPlane ? reinterpret_cast<double*>(smem + L.plane) : gws + static_cast<size_t>(blockIdx.x) * 2 * nn;
+  double* Bpp = A + nn;
   __shared__ int s_bad;
 
   for (int sample = blockIdx.x; sample < nsamples; sample += gridDim.x) {
@@ -113,15 +116,15 @@ __global__ void __launch_bounds__(kMeasThreads)
       continue;
     }
     for (int q = 0; q < m.nqp; ++q) {
-      for (size_t k = tid; k < nn; k += nt) {
-        const int i = static_cast<int>(k / n), j = static_cast<int>(k - static_cast<size_t>(i) * n);
+      for (int k = tid; k < n * n; k += nt) {
+        const int i = k / n, j = k - i * n;
         const int ri = idx[i] + (i >= ne ? ns : 0), rj = idx[j] + (j >= ne ? ns : 0);
         A[k] = __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + ri) * m.ns2 + rj);
       }
       __syncthreads();
       double pfv;
       int st;
-      gj_pfinv<double>(A, n, n, gj, pfv, st);
+      gj_pfinv_pp<double, JPL>(A, Bpp, n, pfv, st);
       if (st != 0) {
         if (tid == 0) s_bad = 1;
         __syncthreads();
@@ -154,8 +157,8 @@ __global__ void __launch_bounds__(kMeasThreads)
       }
       __syncthreads();
       const double cs = pfv * m.spgl[spidx], cc = pfv * m.spgl[m.nleg + spidx], ss = pfv * m.spgl[2 * m.nleg + spidx];
-      for (size_t k = tid; k < nn; k += nt) {
-        const int i = static_cast<int>(k / n), j = static_cast<int>(k - static_cast<size_t>(i) * n);
+      for (int k = tid; k < n * n; k += nt) {
+        const int i = k / n, j = k - i * n;
         const int orb = __ldg(m.orb_idx + tr[i] * ns + tr[j]);
         if (orb < 0 || orb >= m.norb) continue;
         const int sign = sg[i] * sg[j] * __ldg(m.orb_sgn + tr[i] * ns + tr[j]);
@@ -307,29 +310,41 @@ __global__ void k_weight_average(int size, double* tot) {
 
 size_t measure_smem(const DevModel& m, bool smem_plane) { return meas_layout(m, smem_plane).total; }
 
-int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
-                   const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                   double* eloc, int* valid, unsigned* status, cudaStream_t stream) {
-  int dev = 0, limit = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+template <int JPL>
+int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
+                       const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
+                       double* eloc, int* valid, unsigned* status, cudaStream_t stream, int limit) {
   const bool smem_plane = meas_layout(m, true).total <= static_cast<size_t>(limit);
   const size_t smem = meas_layout(m, smem_plane).total;
   if (smem > static_cast<size_t>(limit)) return kErrArgument;
-  int grid = nsamples;
   if (smem_plane) {
-    MVMCB_CUDA(cudaFuncSetAttribute(k_measure<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k_measure<true><<<grid, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws,
-                                                          ostore, eloc, valid, status);
+    auto kernel = k_measure<JPL, true>;
+    MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kernel<<<nsamples, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc,
+                                                     valid, status);
   } else {
-    grid = std::min(nsamples, gws_blocks);
-    MVMCB_CUDA(cudaFuncSetAttribute(k_measure<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k_measure<false><<<grid, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws,
-                                                           ostore, eloc, valid, status);
+    auto kernel = k_measure<JPL, false>;
+    MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kernel<<<std::min(nsamples, gws_blocks), kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples,
+                                                                          gws, ostore, eloc, valid, status);
   }
   MVMCB_CUDA(cudaGetLastError());
   return kOk;
+}
+
+int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
+                   const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
+                   double* eloc, int* valid, unsigned* status, cudaStream_t stream) {
+  int dev = 0, limit = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int n = m.n;
+  if (n <= 32) return launch_measure_jpl<1>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
+  if (n <= 64) return launch_measure_jpl<2>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
+  if (n <= 128) return launch_measure_jpl<4>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
+  if (n <= 224) return launch_measure_jpl<7>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
+  if (n <= 256) return launch_measure_jpl<8>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
+  return kErrArgument;
 }
 
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,

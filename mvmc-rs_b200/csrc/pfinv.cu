@@ -16,6 +16,7 @@
 namespace mvmcb {
 
 constexpr int kPfinvThreads = 256;
+int device_sm_count();
 
 // Column-major X read row-major is Xᵀ = −X, so loading −buffer gives X row-major and the
 // row-major X⁻¹ negated is the column-major X⁻¹.
@@ -59,6 +60,58 @@ __global__ void __launch_bounds__(kPfinvThreads)
     }
     __syncthreads();
   }
+}
+
+// One barrier per pivot step: the matrix and its ping-pong partner in shared memory.
+template <typename T, int JPL>
+__global__ void __launch_bounds__(kPfinvThreads)
+    k_pfinv_pp(const double* __restrict__ x, const int* __restrict__ sizes,
+               const long long* __restrict__ offsets, int n_uniform, int planes, int n_max,
+               double* __restrict__ pf, double* __restrict__ inv, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* A = reinterpret_cast<T*>(smem);
+  T* B = A + static_cast<size_t>(n_max) * n_max;
+  for (int plane = blockIdx.x; plane < planes; plane += gridDim.x) {
+    const int n = sizes ? sizes[plane] : n_uniform;
+    const long long off = offsets ? offsets[plane] : static_cast<long long>(plane) * n * n;
+    const double* xp = x + off;
+    double* ip = inv + off;
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) A[k] = static_cast<T>(-xp[k]);
+    __syncthreads();
+    double pfv;
+    int st;
+    gj_pfinv_pp<T, JPL>(A, B, n, pfv, st);
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) ip[k] = -static_cast<double>(A[k]);
+    if (threadIdx.x == 0) {
+      pf[plane] = pfv;
+      status[plane] = st;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, int JPL>
+int launch_pfinv_pp(const double* x, const int* sizes, const long long* offsets, int n_uniform,
+                    int planes, int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
+  const size_t smem = 2 * sizeof(T) * static_cast<size_t>(n_max) * n_max;
+  auto kernel = k_pfinv_pp<T, JPL>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 0;
+  MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPfinvThreads, smem));
+  const int grid = std::max(1, std::min(planes, std::max(1, per_sm) * device_sm_count()));
+  kernel<<<grid, kPfinvThreads, smem, stream>>>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+template <typename T>
+int dispatch_pfinv_pp(const double* x, const int* sizes, const long long* offsets, int n_uniform,
+                      int planes, int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
+  if (n_max <= 32) return launch_pfinv_pp<T, 1>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  if (n_max <= 64) return launch_pfinv_pp<T, 2>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  if (n_max <= 128) return launch_pfinv_pp<T, 4>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  if (n_max <= 224) return launch_pfinv_pp<T, 7>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  return launch_pfinv_pp<T, 8>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
 }
 
 template <typename T>
@@ -111,6 +164,13 @@ int pfinv_device(const double* x, const int* sizes, const long long* offsets, in
   if (planes <= 0) return kOk;
   if (n_max <= 0 || (n_max & 1) || !x || !pf || !inv || !status) return kErrArgument;
   const int limit = device_smem_limit();
+  const size_t pp_bytes = 2 * static_cast<size_t>(n_max) * n_max * (precision == 32 ? 4 : 8);
+  if (n_max <= 256 && pp_bytes <= static_cast<size_t>(limit)) {
+    if (precision == 32)
+      return dispatch_pfinv_pp<float>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+    if (precision == 64)
+      return dispatch_pfinv_pp<double>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  }
   if (precision == 32) {
     if (pfinv_smem_bytes<float>(n_max, true) > static_cast<size_t>(limit)) return kErrArgument;
     return launch_pfinv<float, true>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status,

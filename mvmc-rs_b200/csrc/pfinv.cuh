@@ -145,3 +145,124 @@ __device__ void gj_pfinv(T* A, int lda, int n, const GJShared<T>& s, double& pf_
 }
 
 }  // namespace mvmcb
+
+namespace mvmcb {
+
+// Ping-pong form of the sweep: one barrier per pivot step. Every warp picks the pivot
+// redundantly from the unmodified source buffer (identical data, identical choice), reads
+// rows p and q from it, and writes the swept matrix into the other buffer. Lane l owns
+// columns j = l + 32c (c < JPL), with the swept flags of its columns in registers.
+// A holds X on entry; the result X⁻¹ is returned in A (B is scratch of the same size).
+// n <= 32·JPL, lda = n. Same pivot rule and status codes as gj_pfinv.
+template <typename T, int JPL>
+__device__ void gj_pfinv_pp(T* A, T* B, int n, double& pf_out, int& status_out) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  unsigned swept = 0;  // bit c: column lane + 32c swept
+  int p = 0, parity = 0, status = 0;
+  double pf = 1.0;
+  T* C = A;
+  T* D = B;
+  for (int k = 0; k < n / 2; ++k) {
+    const T* rowp = C + static_cast<size_t>(p) * n;
+    T rp[JPL];
+    double best = -1.0;
+    int bi = n;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      rp[c] = j < n ? rowp[j] : T(0);
+      if (j < n && j != p && !((swept >> c) & 1u)) {
+        const double v = fabs(static_cast<double>(rp[c]));
+        if (v > best) {
+          best = v;
+          bi = j;
+        }
+      }
+    }
+    warp_argmax_first(best, bi);
+    const int q = __shfl_sync(0xffffffffu, bi, 0);
+    best = __shfl_sync(0xffffffffu, best, 0);
+    if (!(best > 0.0)) {
+      status = p + 1;
+      break;
+    }
+    // parity: unswept columns strictly between p and q
+    int cnt = 0;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      cnt += (j < n && !((swept >> c) & 1u) && j > p && j < q) ? 1 : 0;
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    parity += cnt;
+    const T* rowq = C + static_cast<size_t>(q) * n;
+    const T a = rowp[q];
+    pf *= static_cast<double>(a);
+    const T ia = T(1) / a;
+    T rq[JPL];
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      rq[c] = j < n ? rowq[j] : T(0);
+    }
+    for (int i = warp; i < n; i += nwarp) {
+      const T* Ci = C + static_cast<size_t>(i) * n;
+      T* Di = D + static_cast<size_t>(i) * n;
+      if (i == p) {
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j < n) Di[j] = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
+        }
+      } else if (i == q) {
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j < n) Di[j] = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
+        }
+      } else {
+        const T rpi = rowp[i], rqi = rowq[i];
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j >= n) continue;
+          T v;
+          if (j == p) v = -rqi * ia;
+          else if (j == q) v = rpi * ia;
+          else v = Ci[j] + (rqi * rp[c] - rpi * rq[c]) * ia;
+          Di[j] = v;
+        }
+      }
+    }
+    // mark p, q and find the next pivot row (smallest unswept index)
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j == p || j == q) swept |= 1u << c;
+    }
+    int nxt = n;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j < n && !((swept >> c) & 1u) && j < nxt) nxt = j;
+    }
+    for (int off = 16; off > 0; off >>= 1) nxt = min(nxt, __shfl_xor_sync(0xffffffffu, nxt, off));
+    p = nxt < n ? nxt : 0;
+    __syncthreads();
+    T* t = C;
+    C = D;
+    D = t;
+  }
+  if (C != A && status == 0) {
+    for (int k = tid; k < n * n; k += nt) A[k] = C[k];
+    __syncthreads();
+  }
+  double v = (parity & 1) ? -pf : pf;
+  if (status == 0 && !isfinite(v)) status = -1;
+  if (status != 0) v = 0.0;
+  pf_out = v;
+  status_out = status;
+}
+
+}  // namespace mvmcb

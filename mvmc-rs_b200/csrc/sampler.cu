@@ -56,7 +56,9 @@ __host__ __device__ inline SampLayout samp_layout(const DevModel& m, bool smem_p
   L.vec = o; o = align16(o + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n + sizeof(double) * 8 * m.nqp);
   L.gj = o; o = align16(o + gj_shared_bytes<double>(m.n));
   L.ws = o;
-  if (smem_ws) o = align16(o + sizeof(double) * static_cast<size_t>(m.n) * m.n);
+  // FP64 sweep buffers: two n×n buffers for FP32 planes, one scratch buffer for FP64 planes
+  const size_t nn8 = sizeof(double) * static_cast<size_t>(m.n) * m.n;
+  if (smem_ws) o = align16(o + (sizeof(T) == sizeof(double) ? nn8 : 2 * nn8));
   L.planes = o;
   if (smem_planes) o = align16(o + sizeof(T) * static_cast<size_t>(m.nqp) * m.n * m.n);
   L.total = o;
@@ -90,7 +92,8 @@ struct WalkerSmem {
   T* vec;          // [nqp][4][n]
   double* pscal;   // [nqp][8] per-plane scalars
   GJShared<double> gj;
-  double* ws;      // FP64 refresh workspace (n*n)
+  double* ws;      // FP64 sweep buffer (FP32 planes: the matrix; FP64 planes: the scratch)
+  double* ws2;     // second FP64 sweep buffer (FP32 planes)
   T* planes;       // [nqp][n][n]
 };
 
@@ -163,12 +166,16 @@ __device__ void update_proj_cnt_warp(const DevModel& m, const int* jtab, int ri,
 }
 
 // ---- CalculateMAll on every plane (CTA-wide); returns 0 ok, else the first failure -------
-template <typename T>
+// FP64 planes are swept in place with ws as the ping-pong partner; FP32 planes are swept
+// in FP64 in ws/ws2 and rounded into the plane (the FP64 refresh of the mixed path).
+template <typename T, int JPL>
 __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status) {
   const int n = m.n;
+  const bool fp64_planes = sizeof(T) == sizeof(double);
   int info = 0;
   for (int q = 0; q < m.nqp; ++q) {
-    double* A = s.ws ? s.ws : reinterpret_cast<double*>(s.planes + static_cast<size_t>(q) * n * n);
+    double* A = fp64_planes ? reinterpret_cast<double*>(s.planes + static_cast<size_t>(q) * n * n) : s.ws;
+    double* B = fp64_planes ? s.ws : s.ws2;
     for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
       const int i = k / n, j = k - i * n;
       A[k] = __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + rs_of(m, s.idx, i)) * m.ns2 +
@@ -177,12 +184,12 @@ __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigne
     __syncthreads();
     double pfv;
     int st;
-    gj_pfinv<double>(A, n, n, s.gj, pfv, st);
-    if (s.ws) {
+    gj_pfinv_pp<double, JPL>(A, B, n, pfv, st);
+    if (!fp64_planes) {
       T* P = s.planes + static_cast<size_t>(q) * n * n;
       for (int k = threadIdx.x; k < n * n; k += blockDim.x) P[k] = static_cast<T>(A[k]);
-      __syncthreads();
     }
+    __syncthreads();
     if (st != 0) {
       info = st;
       break;
@@ -518,8 +525,13 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
   s.pscal = reinterpret_cast<double*>(smem + L.vec + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n);
   s.gj = gj_carve<double>(smem + L.gj, m.n);
   const size_t nn = static_cast<size_t>(m.n) * m.n;
-  if (kSmemWs) s.ws = reinterpret_cast<double*>(smem + L.ws);
-  else s.ws = (sizeof(T) == sizeof(double)) ? nullptr : w.ws64 + static_cast<size_t>(wk) * nn;
+  if (kSmemWs) {
+    s.ws = reinterpret_cast<double*>(smem + L.ws);
+    s.ws2 = s.ws + nn;
+  } else {
+    s.ws = w.ws64 + static_cast<size_t>(wk) * 2 * nn;
+    s.ws2 = s.ws + nn;
+  }
   s.planes = kSmemPlanes ? reinterpret_cast<T*>(smem + L.planes)
                          : reinterpret_cast<T*>(w.inv) + static_cast<size_t>(wk) * m.nqp * nn;
 
@@ -552,7 +564,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
     for (int attempt = 1; attempt <= 101; ++attempt) {
       if (tid == 0) make_initial_sample_dev(m, rng, s.idx, s.cfg, s.num, s.cnt);
       __syncthreads();
-      const int info = calc_m_all_dev<T>(m, s, w.status);
+      const int info = calc_m_all_dev<T, JPL>(m, s, w.status);
       if (attempt > 100) {
         if (tid == 0) atomicOr(w.status, kDevInitLoops);
         return;
@@ -561,12 +573,12 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
     }
   };
   if (!burn) initial();
-  calc_m_all_dev<T>(m, s, w.status);
+  calc_m_all_dev<T, JPL>(m, s, w.status);
   if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
   __syncthreads();
   if (!isfinite(s.dctl[dLogIp])) {
     initial();
-    calc_m_all_dev<T>(m, s, w.status);
+    calc_m_all_dev<T, JPL>(m, s, w.status);
     if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
     burn = false;
     __syncthreads();
@@ -598,6 +610,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
       int* const cc = s.ctl + ((proposal & 1) ? 16 : 0);
       // --- candidate (thread 0) ---
       if (tid == 0) {
+        ++since_refresh;  // proposal attempts since the last FP64 refresh (mixed path)
         int type;
         switch (m.nex_path) {
           case 0: type = 0; break;
@@ -721,13 +734,13 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
           revert_electron(m, s.idx, s.cfg, s.num, cc[cMi], ri, rj, sp);
         }
         cc[cAccept] = acc;
-        ++since_refresh;
         int refresh = 0;
-        if (n_acc_win > ns) {
-          refresh = 1;
+        if (refresh_every > 0) {
+          // mixed path: FP64 refresh of Pf and X⁻¹ every NRefresh sweeps
+          if (since_refresh >= refresh_every) refresh = 2;
+        } else if (n_acc_win > ns) {
+          refresh = 1;  // C rule: recompute when the accept window exceeds Nsite
           n_acc_win = 0;
-        } else if (refresh_every > 0 && since_refresh >= refresh_every) {
-          refresh = 2;  // extra FP64 refresh of the mixed path (does not reset the C window)
         }
         if (refresh) since_refresh = 0;
         cc[cRefresh] = refresh;
@@ -743,7 +756,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
       }
       lap(kPhUpdate);
       if (cc[cRefresh]) {
-        const int info = calc_m_all_dev<T>(m, s, w.status);
+        const int info = calc_m_all_dev<T, JPL>(m, s, w.status);
         if (tid == 0 && info == 0 && cc[cRefresh] == 1) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
         if (tid == 0 && info == 0 && cc[cRefresh] == 2) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
         __syncthreads();
@@ -802,7 +815,7 @@ bool sample_planes_in_smem(const DevModel& m, int precision, int limit) {
   if (residency_policy() == 1) return false;
   if (precision == 32) return samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit) ||
                               samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit);
-  return samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit);
+  return samp_layout<double>(m, true, true).total <= static_cast<size_t>(limit);
 }
 
 // Plane residency: "shared" keeps a walker's planes in shared memory (one walker per SM
@@ -834,8 +847,8 @@ int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int
       return launch_sample_t<float, JPL, 512, true, false>(m, w, stream);
     return launch_sample_t<float, JPL, 256, false, false>(m, w, stream);
   }
-  if (samp_layout<double>(m, true, false).total <= static_cast<size_t>(limit))
-    return launch_sample_t<double, JPL, 512, true, false>(m, w, stream);
+  if (samp_layout<double>(m, true, true).total <= static_cast<size_t>(limit))
+    return launch_sample_t<double, JPL, 512, true, true>(m, w, stream);
   return launch_sample_t<double, JPL, 256, false, false>(m, w, stream);
 }
 

@@ -206,31 +206,37 @@ __device__ void gj_pfinv_pp(T* A, T* B, int n, double& pf_out, int& status_out) 
       const int j = lane + 32 * c;
       rq[c] = j < n ? rowq[j] : T(0);
     }
-    for (int i = warp; i < n; i += nwarp) {
-      const T* Ci = C + static_cast<size_t>(i) * n;
-      T* Di = D + static_cast<size_t>(i) * n;
-      if (i == p) {
+    constexpr int RB = 4;  // rows per batch: their loads are issued before any store
+    for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
+      T ci[RB][JPL];
+      T rpi[RB], rqi[RB];
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        const T* Ci = C + static_cast<size_t>(i) * n;
+        rpi[r] = i < n ? rowp[i] : T(0);
+        rqi[r] = i < n ? rowq[i] : T(0);
 #pragma unroll
         for (int c = 0; c < JPL; ++c) {
           const int j = lane + 32 * c;
-          if (j < n) Di[j] = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
+          ci[r][c] = (i < n && j < n) ? Ci[j] : T(0);
         }
-      } else if (i == q) {
+      }
 #pragma unroll
-        for (int c = 0; c < JPL; ++c) {
-          const int j = lane + 32 * c;
-          if (j < n) Di[j] = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
-        }
-      } else {
-        const T rpi = rowp[i], rqi = rowq[i];
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        if (i >= n) continue;
+        T* Di = D + static_cast<size_t>(i) * n;
 #pragma unroll
         for (int c = 0; c < JPL; ++c) {
           const int j = lane + 32 * c;
           if (j >= n) continue;
           T v;
-          if (j == p) v = -rqi * ia;
-          else if (j == q) v = rpi * ia;
-          else v = Ci[j] + (rqi * rp[c] - rpi * rq[c]) * ia;
+          if (i == p) v = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
+          else if (i == q) v = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
+          else if (j == p) v = -rqi[r] * ia;
+          else if (j == q) v = rpi[r] * ia;
+          else v = ci[r][c] + (rqi[r] * rp[c] - rpi[r] * rq[c]) * ia;
           Di[j] = v;
         }
       }

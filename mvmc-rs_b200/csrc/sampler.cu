@@ -220,6 +220,43 @@ __device__ void ratio_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa
   }
 }
 
+// Column-form product over plane rows with independent accumulators so that several
+// row loads are in flight: out = Σ_i P[i·n + col]·v[i] (P points at the column).
+template <typename T>
+__device__ __forceinline__ T col_dot(const T* __restrict__ P, const T* __restrict__ v, int n) {
+  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+  int i = 0;
+  for (; i + 4 <= n; i += 4) {
+    a0 += P[(i + 0) * n] * v[i + 0];
+    a1 += P[(i + 1) * n] * v[i + 1];
+    a2 += P[(i + 2) * n] * v[i + 2];
+    a3 += P[(i + 3) * n] * v[i + 3];
+  }
+  for (; i < n; ++i) a0 += P[i * n] * v[i];
+  return (a0 + a1) + (a2 + a3);
+}
+
+template <typename T>
+__device__ __forceinline__ void col_dot2(const T* __restrict__ P, const T* __restrict__ v,
+                                         const T* __restrict__ u, int n, T& pv, T& pu) {
+  T a0 = T(0), a1 = T(0), b0 = T(0), b1 = T(0);
+  int i = 0;
+  for (; i + 2 <= n; i += 2) {
+    const T x0 = P[i * n], x1 = P[(i + 1) * n];
+    a0 += x0 * v[i];
+    b0 += x0 * u[i];
+    a1 += x1 * v[i + 1];
+    b1 += x1 * u[i + 1];
+  }
+  for (; i < n; ++i) {
+    const T x = P[i * n];
+    a0 += x * v[i];
+    b0 += x * u[i];
+  }
+  pv = a0 + a1;
+  pu = b0 + b1;
+}
+
 // Lane-owned columns: lane l of every warp owns columns j = l + 32c (c < JPL) of every
 // plane row it touches, so column vectors of the rank-2/rank-4 updates sit in registers
 // and only the row scalars are broadcast from shared memory.
@@ -241,11 +278,7 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
   for (int k = tid; k < nq * n; k += nt) {  // column form: one thread per (plane, column)
     const int q = k / n, j = k - q * n;
     const T* P = s.planes + static_cast<size_t>(q) * n * n + j;
-    const T* slt = vec + (q * 4 + 0) * n;
-    T acc = T(0);
-#pragma unroll 8
-    for (int i = 0; i < n; ++i) acc += -P[i * n] * slt[i];
-    vec[(q * 4 + 1) * n + j] = acc;
+    vec[(q * 4 + 1) * n + j] = -col_dot(P, vec + (q * 4 + 0) * n, n);
   }
   __syncthreads();
   for (int k = tid; k < nq * n; k += nt) {
@@ -268,17 +301,40 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
       v2c[c] = j < n ? v2[j] : T(0);
     }
     T* P = s.planes + static_cast<size_t>(q) * n * n;
-    for (int i = warp; i < n; i += nwarp) {
-      const T v1i = v1[i], v2i = v2[i];
-      T* Pi = P + static_cast<size_t>(i) * n;
-      if (i != msa) {
+    constexpr int RB = 4;  // rows per batch: their loads are issued before any store
+    for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
+      T x[RB][JPL];
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
 #pragma unroll
         for (int c = 0; c < JPL; ++c) {
           const int j = lane + 32 * c;
-          if (j < n) Pi[j] = Pi[j] + (v1i * v2c[c] - v1c[c] * v2i);
+          x[r][c] = (i < n && j < n) ? P[static_cast<size_t>(i) * n + j] : T(0);
         }
-        if (lane == lmsa) Pi[msa] -= v2i;  // the thread that owns column msa of this row
-      } else {
+      }
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        if (i >= n || i == msa) continue;
+        const T v1i = v1[i], v2i = v2[i];
+        T* Pi = P + static_cast<size_t>(i) * n;
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j < n) {
+            T y = x[r][c] + (v1i * v2c[c] - v1c[c] * v2i);
+            if (c == cmsa && lane == lmsa) y -= v2i;  // column msa of this row
+            Pi[j] = y;
+          }
+        }
+      }
+    }
+    for (int i = warp; i < n; i += nwarp) {
+      if (i != msa) continue;
+      const T v1i = v1[i], v2i = v2[i];
+      T* Pi = P + static_cast<size_t>(i) * n;
+      {
 #pragma unroll
         for (int c = 0; c < JPL; ++c) {
           const int j = lane + 32 * c;
@@ -313,11 +369,7 @@ __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, in
   for (int k = tid; k < nq * n; k += nt) {
     const int q = k / n, i = k - q * n;
     const T* P = s.planes + static_cast<size_t>(q) * n * n + i;
-    const T* va = vec + (q * 4 + 0) * n;
-    T t = T(0);
-#pragma unroll 8
-    for (int j = 0; j < n; ++j) t += P[j * n] * va[j];
-    vec[(q * 4 + 2) * n + i] = -t;
+    vec[(q * 4 + 2) * n + i] = -col_dot(P, vec + (q * 4 + 0) * n, n);
   }
   __syncthreads();
   for (int q = warp; q < nq; q += nwarp) {
@@ -365,15 +417,8 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
   for (int k = tid; k < nq * n; k += nt) {
     const int q = k / n, i = k - q * n;
     const T* P = s.planes + static_cast<size_t>(q) * n * n + i;
-    const T* vs = vec + (q * 4 + 0) * n;
-    const T* vt = vec + (q * 4 + 1) * n;
-    T p = T(0), r = T(0);
-#pragma unroll 8
-    for (int j = 0; j < n; ++j) {
-      const T x = P[j * n];
-      p += x * vs[j];
-      r += x * vt[j];
-    }
+    T p, r;
+    col_dot2(P, vec + (q * 4 + 0) * n, vec + (q * 4 + 1) * n, n, p, r);
     vec[(q * 4 + 2) * n + i] = -p;
     vec[(q * 4 + 3) * n + i] = -r;
   }
@@ -427,7 +472,22 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
       tc[c2] = j < n ? vt[j] : T(0);
     }
     T* P = s.planes + static_cast<size_t>(q) * n * n;
-    for (int i = warp; i < n; i += nwarp) {
+    constexpr int RB = 2;  // rows per batch: their loads are issued before any store
+    for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
+     T xl[RB][JPL];
+#pragma unroll
+     for (int r = 0; r < RB; ++r) {
+       const int i = i0 + r * nwarp;
+#pragma unroll
+       for (int c2 = 0; c2 < JPL; ++c2) {
+         const int j = lane + 32 * c2;
+         xl[r][c2] = (i < n && j < n) ? P[static_cast<size_t>(i) * n + j] : T(0);
+       }
+     }
+#pragma unroll
+     for (int r = 0; r < RB; ++r) {
+      const int i = i0 + r * nwarp;
+      if (i >= n) continue;
       const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
       T* Pi = P + static_cast<size_t>(i) * n;
       const bool row_fix = (i == msa) || (i == msb);
@@ -436,7 +496,7 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
         const int j = lane + 32 * c2;
         if (j >= n) continue;
         const T pj = pc[c2], qj = qc[c2], sj = sc_[c2], tj = tc[c2];
-        T x = Pi[j] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
+        T x = xl[r][c2] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
                        d * (pi * sj - pj * si) + edet * (si * tj - sj * ti) + fidet * (pi * qj - qi * pj));
         if (j == msa) x += -c * ti - d * si - fidet * qi;
         if (j == msb) x += -a * ti - b * si + fidet * pi;
@@ -448,6 +508,7 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
         }
         Pi[j] = x;
       }
+     }
     }
   }
   __syncthreads();

@@ -170,7 +170,9 @@ def test_full_optimisation_matches_oracle_zvo_out(tmp_path):
     assert np.all(np.abs(a[:, 0] - b[:, 0]) <= 1e-6 * np.abs(b[:, 0]))
     va = read_out(gdir / "zvo_var.dat")
     vb = read_out(odir / "zvo_var.dat")
-    assert np.allclose(va, vb, rtol=1e-6, atol=1e-7)
+    # parameters after each step, relative to the largest parameter of the step
+    scale = np.abs(vb).max(axis=1, keepdims=True)
+    assert np.all(np.abs(va - vb) <= 1e-6 * scale)
     for name in ("zqp_opt.dat", "zvo_SRinfo.dat", "zqp_orbital_opt.dat"):
         assert (gdir / name).exists() and (odir / name).exists()
     sa = [l.split() for l in open(gdir / "zvo_SRinfo.dat").read().splitlines()[1:]]

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(kMeasThreads)
       __syncthreads();
       double pfv;
       int st;
-      gj_pfinv_pp<double, JPL>(A, Bpp, n, pfv, st);
+      gj_pfinv_pp<double, JPL, kSmemPlane ? 1 : 4>(A, Bpp, n, pfv, st);
       if (st != 0) {
         if (tid == 0) s_bad = 1;
         __syncthreads();

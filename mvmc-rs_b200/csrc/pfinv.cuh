@@ -154,7 +154,7 @@ namespace mvmcb {
 // columns j = l + 32c (c < JPL), with the swept flags of its columns in registers.
 // A holds X on entry; the result X⁻¹ is returned in A (B is scratch of the same size).
 // n <= 32·JPL, lda = n. Same pivot rule and status codes as gj_pfinv.
-template <typename T, int JPL>
+template <typename T, int JPL, int RB = 1>
 __device__ void gj_pfinv_pp(T* A, T* B, int n, double& pf_out, int& status_out) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
@@ -206,7 +206,8 @@ __device__ void gj_pfinv_pp(T* A, T* B, int n, double& pf_out, int& status_out) 
       const int j = lane + 32 * c;
       rq[c] = j < n ? rowq[j] : T(0);
     }
-    constexpr int RB = 4;  // rows per batch: their loads are issued before any store
+    // RB rows per batch: their loads are issued before any store (RB > 1 for buffers in
+    // global memory, where each row costs an L2 round trip)
     for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
       T ci[RB][JPL];
       T rpi[RB], rqi[RB];

@@ -168,7 +168,7 @@ __device__ void update_proj_cnt_warp(const DevModel& m, const int* jtab, int ri,
 // ---- CalculateMAll on every plane (CTA-wide); returns 0 ok, else the first failure -------
 // FP64 planes are swept in place with ws as the ping-pong partner; FP32 planes are swept
 // in FP64 in ws/ws2 and rounded into the plane (the FP64 refresh of the mixed path).
-template <typename T, int JPL>
+template <typename T, int JPL, bool kGlobalSweep>
 __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status) {
   const int n = m.n;
   const bool fp64_planes = sizeof(T) == sizeof(double);
@@ -184,7 +184,8 @@ __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigne
     __syncthreads();
     double pfv;
     int st;
-    gj_pfinv_pp<double, JPL>(A, B, n, pfv, st);
+    if (kGlobalSweep) gj_pfinv_pp<double, JPL, 4>(A, B, n, pfv, st);
+    else gj_pfinv_pp<double, JPL, 1>(A, B, n, pfv, st);
     if (!fp64_planes) {
       T* P = s.planes + static_cast<size_t>(q) * n * n;
       for (int k = threadIdx.x; k < n * n; k += blockDim.x) P[k] = static_cast<T>(A[k]);
@@ -625,7 +626,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
     for (int attempt = 1; attempt <= 101; ++attempt) {
       if (tid == 0) make_initial_sample_dev(m, rng, s.idx, s.cfg, s.num, s.cnt);
       __syncthreads();
-      const int info = calc_m_all_dev<T, JPL>(m, s, w.status);
+      const int info = calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
       if (attempt > 100) {
         if (tid == 0) atomicOr(w.status, kDevInitLoops);
         return;
@@ -634,12 +635,12 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
     }
   };
   if (!burn) initial();
-  calc_m_all_dev<T, JPL>(m, s, w.status);
+  calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
   if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
   __syncthreads();
   if (!isfinite(s.dctl[dLogIp])) {
     initial();
-    calc_m_all_dev<T, JPL>(m, s, w.status);
+    calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
     if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
     burn = false;
     __syncthreads();
@@ -817,7 +818,7 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
       }
       lap(kPhUpdate);
       if (cc[cRefresh]) {
-        const int info = calc_m_all_dev<T, JPL>(m, s, w.status);
+        const int info = calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
         if (tid == 0 && info == 0 && cc[cRefresh] == 1) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
         if (tid == 0 && info == 0 && cc[cRefresh] == 2) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
         __syncthreads();

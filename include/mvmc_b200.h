@@ -123,6 +123,23 @@ int mvmc_b200_cg_solve(const double* samples, long long ns, int na, const double
                        const double* diag, const double* g, double inv_w, double shift, double tol,
                        int max_iter, int diag_scale, double* x, long long* status);
 
+/* SR-CG on device buffers without any device allocation. This entry point has no
+ * counterpart in the reference: it serves callers whose device memory is owned by their
+ * own allocator (a pooling framework allocator, a fixed memory budget), where a library
+ * cudaMalloc would fragment the pool or overrun the budget and cudaMalloc/cudaFree would
+ * synchronise the device. All pointers are device pointers: samples [ns][na] row-major,
+ * mean/diag/g [na] inputs; x [na] and result [3] = {delta, status, iterations} outputs.
+ * The working vectors live in an 8 MiB array compiled into the library (held on every
+ * GPU that loads it until exit); problems needing more than 1048576 doubles of it
+ * (3·na + ns + column partials) return MVMC_B200_EARG with a message. The first call on
+ * a device looks up that array's device address; make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be serialised.
+ * stream is a cudaStream_t (NULL = default); the call returns once the solve is queued. */
+int mvmc_b200_cg_solve_noalloc(const double* samples, long long ns, int na, const double* mean,
+                               const double* diag, const double* g, double inv_w, double shift,
+                               double tol, int max_iter, int diag_scale, double* x, double* result,
+                               void* stream);
+
 /* Sticky device status word (first failing stage wins): MVMC_B200_DEV_* bits. */
 #define MVMC_B200_DEV_SINGULAR 1u
 #define MVMC_B200_DEV_NONFINITE 2u

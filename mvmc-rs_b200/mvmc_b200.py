@@ -20,7 +20,7 @@ EXPORTS = [
     "mvmc_b200_get_samples", "mvmc_b200_measure", "mvmc_b200_get_o_store",
     "mvmc_b200_get_local_energies", "mvmc_b200_sr_cg", "mvmc_b200_status", "mvmc_b200_run_opt",
     "mvmc_b200_last_error", "mvmc_b200_cg_solve", "mvmc_b200_stream", "mvmc_b200_transfer_bytes",
-    "mvmc_b200_sampler_timers",
+    "mvmc_b200_sampler_timers", "mvmc_b200_cg_solve_noalloc",
 ]
 
 
@@ -88,6 +88,17 @@ def cg_solve(samples, mean, diag, g, inv_w, shift, tol, max_iter, diag_scale=Fal
                                     ctypes.c_double(inv_w), ctypes.c_double(shift), ctypes.c_double(tol),
                                     max_iter, int(diag_scale), _ptr(x), ctypes.byref(st)), "cg_solve")
     return st.value, x
+
+
+def cg_solve_noalloc(samples_ptr, ns, na, mean_ptr, diag_ptr, g_ptr, inv_w, shift, tol, max_iter,
+                     diag_scale, x_ptr, result_ptr, stream=0):
+    """SR-CG on device buffers (integer device addresses) with no device allocation by the
+    library; result_ptr receives {delta, status, iterations}. Returns the C status code."""
+    vp = ctypes.c_void_p
+    return _check(lib().mvmc_b200_cg_solve_noalloc(
+        vp(samples_ptr), ctypes.c_longlong(ns), na, vp(mean_ptr), vp(diag_ptr), vp(g_ptr),
+        ctypes.c_double(inv_w), ctypes.c_double(shift), ctypes.c_double(tol), max_iter, int(diag_scale),
+        vp(x_ptr), vp(result_ptr), vp(stream)), "cg_solve_noalloc")
 
 
 def default_options(**kw):

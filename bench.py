@@ -1,28 +1,42 @@
-"""Benchmark: one VMC optimisation step (resident sampling → measurement → SR-CG) per
-timed step, on the synthetic Hubbard workloads of mvmc-rs_b200/lattice.py.
+"""Benchmark of the VMC sampling + SR hot path on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config square8]
-                    [--precision 64|32] [--impl ours|reference]
+                    [--precision 32|64] [--impl ours|reference]
 
-Prints one JSON line (rank 0). `value` is Metropolis sweeps/s of the whole job with the
-model resident on the device; `e2e` times the same steps through the public C ABI calls
-including their host↔device copies. For N > 1 (torchrun) every rank runs its own walker
+Engine workloads (chain16, square8, square16, square16_sr; mvmc-rs_b200/lattice.py): a
+step is one SR step — resident sampling (burn-in chain of NVMCSample + 1 blocks of
+NVMCInterval sweeps per walker), measurement with the adjoint O rows, SR-CG and the
+parameter update. `value` is Metropolis sweeps/s of the whole job with the model resident
+on the device. The default line is the plain FP64 path; the mixed path (FP32 inverse
+updates, FP64 refresh every --refresh sweeps and after guard-tripping moves) is timed
+beside it on the same workload and seeds (`mixed_path`), and `accuracy` compares one
+fresh sample + measurement of the two.
+
+Pfaffian workloads (pfinv64, pfinv_mix): a step is one batched Pfaffian + inverse launch
+over B = 8192 (8190 for the five-size mix) seeded skew planes; `value` is planes/s.
+
+`e2e` times the same steps through the public C ABI calls with host buffers, host↔device
+copies inside the timed region. For N > 1 (torchrun) every rank runs its own walker
 ensemble (seeds offset by rank × walkers): replicas, no data-path collective.
 """
 import argparse
-import ctypes
 import json
 import os
+import statistics
 import subprocess
 import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "mvmc-rs_b200"))
 
 WALKERS = {"chain16": 256, "square8": 4096, "square16": 2048, "square16_sr": 8192}
+PFINV = {"pfinv64": [64] * 8192, "pfinv_mix": [32, 48, 64, 96, 128] * 1638}
 METRIC = "Metropolis sweeps/s & SR-step time: mixed vs FP64 path on 1 B200 at |dE|/N<=1e-6"
+PFINV_METRIC = "Pfaffian+inverse/s (batched skew FP64)"
 
 
 def measured_peaks():
@@ -45,8 +59,13 @@ def start_clock_sampler(path):
         return None
 
 
+def stop_clock_sampler(sampler):
+    if sampler is not None:
+        sampler.terminate()
+        sampler.wait()
+
+
 def summarize_clocks(path, device):
-    import statistics
     rows = []
     try:
         for line in open(path):
@@ -66,7 +85,7 @@ def summarize_clocks(path, device):
                 reasons.add(name)
     return {"sm_mhz": statistics.median(sm) if sm else None,
             "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
-            "reasons": sorted(reasons)}
+            "reasons": sorted(reasons), "samples": len(rows)}
 
 
 def dist_env():
@@ -76,29 +95,449 @@ def dist_env():
     return ws, rank, local
 
 
-def cpu_baseline(namelist, initial_def, walkers_per_proc, procs, seconds_hint=10.0):
-    """The oracle (C++ restatement of the reference CPU path) on host cores."""
+# ----------------------------------------------------------------------------------------
+# CPU legs: the oracle (C++ restatement of the reference CPU path) on the host cores.
+# ----------------------------------------------------------------------------------------
+def _oracle_lib():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
     ol.lib()
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
+    return ol
+
+
+def _engine_job(args):
+    namelist, initial_def, walkers, seed = args
+    _oracle_lib().opt_step1_walkers(namelist, walkers, seed=seed, initial_def=initial_def)
+    return 0
+
+
+_PF_DATA = []
+
+
+def _pfinv_init(sizes, per):
+    """Worker set-up: this process's own seeded planes (generated once, not timed)."""
+    global _PF_DATA
+    _oracle_lib()
+    rng = np.random.default_rng(os.getpid())
+    _PF_DATA = [(skew_planes(rng, n, per).ravel(), n, per) for n in sorted(set(sizes))]
+
+
+def _pfinv_job(_):
+    ol = _oracle_lib()
+    for x, n, per in _PF_DATA:
+        ol.pfinv_batch(x, n, per)
+    return 0
+
+
+class CpuPool:
+    """One oracle process per host core (spawned before any GPU work, so no process is
+    forked from a CUDA context); only the map over the jobs is timed."""
+
+    def __init__(self, procs, initializer=None, initargs=()):
+        import multiprocessing as mp
+        self.procs = procs
+        self.pool = mp.get_context("spawn").Pool(procs, initializer=initializer, initargs=initargs)
+
+    def time(self, fn, jobs):
+        t0 = time.perf_counter()
+        self.pool.map(fn, jobs, chunksize=1)
+        return time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_engine_time(namelist, initial_def, walkers):
+    """One process, `walkers` chains of one SR step of the oracle."""
+    _oracle_lib()
     t0 = time.perf_counter()
-    if procs == 1:
-        _oracle_chunk((namelist, initial_def, walkers_per_proc, 12345))
-    else:
-        with ctx.Pool(procs) as pool:
-            pool.map(_oracle_chunk, [(namelist, initial_def, walkers_per_proc, 12345 + k * walkers_per_proc)
-                                     for k in range(procs)])
+    _engine_job((namelist, initial_def, walkers, 12345))
     return time.perf_counter() - t0
 
 
-def _oracle_chunk(args):
-    namelist, initial_def, walkers, seed = args
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib as ol
-    ol.opt_step1_walkers(namelist, walkers, seed=seed, initial_def=initial_def)
-    return 0
+def cpu_pfinv_time(sizes, per):
+    """One process, `per` planes of each size."""
+    _pfinv_init(sizes, per)
+    t0 = time.perf_counter()
+    _pfinv_job(0)
+    return time.perf_counter() - t0
+
+
+def skew_planes(rng, n, planes):
+    """A_ij ~ N(0,1) for i < j, A_ji = -A_ij, plus 0.5·J (J = diag of [[0,1],[-1,0]] blocks);
+    column-major planes (the transpose of a skew matrix is its negative, so the row-major
+    draw is stored negated)."""
+    u = np.triu(rng.standard_normal((planes, n, n)), 1)
+    x = u - np.transpose(u, (0, 2, 1))
+    i = np.arange(0, n, 2)
+    x[:, i, i + 1] += 0.5
+    x[:, i + 1, i] -= 0.5
+    return np.ascontiguousarray(np.transpose(x, (0, 2, 1)))
+
+
+# ----------------------------------------------------------------------------------------
+# Engine workloads.
+# ----------------------------------------------------------------------------------------
+def engine_inputs(args, rank):
+    import lattice
+    cfg = dict(lattice.CONFIGS[args.config])
+    if args.interval:
+        cfg["interval"] = args.interval
+    tmp = tempfile.mkdtemp(prefix=f"mvmc_bench_{rank}_")
+    namelist, initial_def, dims = lattice.write_inputs(os.path.join(tmp, "in"), **cfg)
+    return cfg, tmp, namelist, initial_def, dims
+
+
+def reference_engine(args):
+    cfg, tmp, namelist, initial_def, dims = engine_inputs(args, 0)
+    procs = os.cpu_count() or 1
+    per = 64 if args.config == "chain16" else 2
+    S = cfg["samples"]
+    sweeps = procs * per * (cfg["warmup"] + S) * cfg["interval"]  # the oracle's step 1 runs warm-up + S blocks
+    pool = CpuPool(procs, initializer=_oracle_lib)
+    jobs = [(namelist, initial_def, per, 12345 + k * per) for k in range(procs)]
+    for _ in range(args.warmup):
+        pool.time(_engine_job, jobs)
+    times = [pool.time(_engine_job, jobs) for _ in range(args.steps)]
+    pool.close()
+    t = sum(times) / len(times)
+    value = sweeps / t
+    return {"metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config, "walkers": procs * per,
+                       "sweeps_per_walker": (cfg["warmup"] + S) * cfg["interval"]},
+            "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": procs, "kind": "port",
+                             "sample": f"{procs * per} chains x one SR step (warm-up + {S} sample blocks) "
+                                       f"of {args.config}, one process per core"},
+            "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def time_engine(args, precision, W, namelist, initial_def, cfg, dims, rank, local, ws, dist, timed_hook=None,
+                sr_precision=0):
+    """Warm-up + K timed SR steps of one engine; returns the timing record."""
+    import torch
+    import mvmc_b200 as mb
+    eng = mb.Engine(namelist, initial_def, walkers=W, precision=precision, seed=12345 + rank * W,
+                    device=local, refresh_sweeps=args.refresh if precision == 32 else 0,
+                    refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision)
+    stream = torch.cuda.ExternalStream(eng.stream())
+    energy = None
+    for _ in range(args.warmup):
+        eng.sample()
+        eng.measure()
+        eng.sr_cg()
+    torch.cuda.synchronize()
+    if timed_hook:
+        timed_hook("start")
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    marks = []
+    h0, d0 = eng.transfer_bytes()
+    t_wall0 = time.perf_counter()
+    ev0.record(stream)
+    cg_iters = []
+    for _ in range(args.steps):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        eng.sample()
+        b.record(stream)
+        e, ho, oo = eng.measure()
+        c.record(stream)
+        rc, sri = eng.sr_cg()
+        energy = float(e[1])
+        cg_iters.append(int(sri[8]))
+        marks.append((a, b, c))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall0
+    if timed_hook:
+        timed_hook("stop")
+    h1, d1 = eng.transfer_bytes()
+    ms = ev0.elapsed_time(ev1)
+    samp = [a.elapsed_time(b) for a, b, _ in marks]
+    meas = [b.elapsed_time(c) for _, b, c in marks]
+    if ws > 1:
+        t = torch.tensor([ms, t_wall * 1e3], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, t_wall_ms = float(t[0]), float(t[1])
+    else:
+        t_wall_ms = t_wall * 1e3
+    samples = eng.samples()
+    c = samples["counter"].reshape(-1, 6).sum(axis=0)
+    drift = eng.refresh_stats()
+    eng.close()
+    return {"ms": ms, "t_wall_ms": t_wall_ms, "sample_ms": sum(samp) / len(samp),
+            "measure_ms": sum(meas) / len(meas), "h2d": h1 - h0, "d2h": d1 - d0, "energy": energy,
+            "acceptance": (c[1] + c[3]) / max(1, c[0] + c[2]), "cg_iters": cg_iters, "drift": drift}
+
+
+def accuracy_check(args, W, namelist, initial_def, local):
+    """One fresh sample + measurement of the mixed and the plain FP64 path with the same
+    seeds and parameters: chains that saw no Metropolis decision flip hold identical
+    configurations (and energies to FP64 rounding, since measurement is FP64)."""
+    import mvmc_b200 as mb
+    out = {}
+    for prec in (64, 32):
+        eng = mb.Engine(namelist, initial_def, walkers=W, precision=prec, seed=12345, device=local,
+                        refresh_sweeps=args.refresh if prec == 32 else 0,
+                        refresh_guard=args.guard if prec == 32 else 0.0)
+        eng.sample()
+        e, _, _ = eng.measure()
+        out[prec] = (e, eng.samples()["ele_idx"].reshape(W, -1), eng.local_energies(), eng.refresh_stats())
+        eng.close()
+    e64, idx64, el64, _ = out[64]
+    e32, idx32, el32, drift = out[32]
+    same = np.all(idx64 == idx32, axis=1)
+    return {"walkers": W, "identical_chains": float(same.mean()),
+            "energy_fp64": float(e64[1]), "energy_mixed": float(e32[1]),
+            "dE": float(e32[1] - e64[1]),
+            "stat_err": float(np.std(el64) / np.sqrt(len(el64))),
+            "max_dEloc_identical": float(np.max(np.abs(el64[same] - el32[same]), initial=0.0)),
+            "refresh_drift_max": drift["drift_max"], "refresh_drift_mean": drift["drift_mean"]}
+
+
+def engine_bench(args, ws, rank, local):
+    import torch
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    cfg, tmp, namelist, initial_def, dims = engine_inputs(args, rank)
+    W = args.walkers or WALKERS[args.config]
+    S = cfg["samples"]
+    sweeps_per_walker_step = (S + 1) * cfg["interval"]
+    clocks_path = os.path.join(tmp, "clocks.csv")
+    state = {}
+
+    def hook(what):
+        if rank != 0:
+            return
+        if what == "start":
+            state["sampler"] = start_clock_sampler(clocks_path)
+        else:
+            stop_clock_sampler(state.pop("sampler", None))
+
+    main_rec = time_engine(args, args.precision, W, namelist, initial_def, cfg, dims, rank, local, ws, dist, hook,
+                           sr_precision=args.sr_precision)
+    other = None
+    other_prec = 32 if args.precision == 64 else 64
+    if not args.no_compare:
+        other = time_engine(args, other_prec, W, namelist, initial_def, cfg, dims, rank, local, ws, dist,
+                            sr_precision=args.sr_precision)
+    sweeps_total = ws * W * sweeps_per_walker_step * args.steps
+    value = sweeps_total / (main_rec["ms"] / 1e3)
+    n, nqp, ns = dims["n"], dims["nqp"], dims["nsite"]
+    s_bytes = 8 if args.precision == 64 else 4
+    p_acc = main_rec["acceptance"]
+    # algorithmic bytes per walker-sweep of the resident sampler (InvM row + gathered Slater
+    # row per proposal, rank-2 read+write per accepted move)
+    per_sweep = ns * (nqp * n * s_bytes + nqp * n * 8) + ns * p_acc * nqp * (2 * n * n * s_bytes)
+    launch_bytes = W * sweeps_per_walker_step * per_sweep
+    achieved = launch_bytes / (main_rec["sample_ms"] / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return
+    acc = accuracy_check(args, min(W, 1024), namelist, initial_def, local) if other else None
+    base_t = cpu_engine_time(namelist, initial_def, 1)
+    base_sweeps = (cfg["warmup"] + S) * cfg["interval"]
+    out = {
+        "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": main_rec["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == 64 else "f32+f64refresh", "data": "synthetic",
+        "config": {"workload": args.config, "walkers_per_gpu": W, "nsite": ns, "n": n, "nqp": nqp,
+                   "npara": dims["npara"], "sweeps_per_walker_step": sweeps_per_walker_step,
+                   "precision": args.precision, "parallelism": f"replicas{ws}",
+                   "refresh_sweeps": args.refresh if args.precision == 32 else None,
+                   "refresh_guard": args.guard if args.precision == 32 else None,
+                   "sr_precision": args.sr_precision or 64,
+                   "l2": "inputs larger than L2 between steps (walker planes + O matrix)"},
+        "sr_step_ms": main_rec["ms"] / args.steps, "sample_ms": main_rec["sample_ms"],
+        "measure_ms": main_rec["measure_ms"], "energy": main_rec["energy"], "acceptance": p_acc,
+        "cg_iterations": main_rec["cg_iters"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_sample",
+                     "peak_kind": peak_kind},
+        "cpu_baseline": {"value": base_sweeps / base_t, "unit": "sweeps/s", "cores": 1, "kind": "port",
+                         "sample": f"1 chain x one SR step (warm-up + {S} blocks, {base_sweeps} sweeps) "
+                                   f"of {args.config}"},
+        "e2e": {"value": sweeps_total / (main_rec["t_wall_ms"] / 1e3), "unit": "sweeps/s",
+                "h2d_bytes_per_step": main_rec["h2d"] // args.steps,
+                "d2h_bytes_per_step": main_rec["d2h"] // args.steps},
+        "gpu_launches": 8 * args.steps,
+        "residency": os.environ.get("MVMC_B200_RESIDENCY", "auto"),
+        "clocks": summarize_clocks(clocks_path, local),
+    }
+    if args.precision == 32:
+        out["refresh"] = {"sweeps": args.refresh, "guard": args.guard, **main_rec["drift"]}
+    if other:
+        rec = {"precision": other_prec, "value": sweeps_total / (other["ms"] / 1e3),
+               "sr_step_ms": other["ms"] / args.steps, "sample_ms": other["sample_ms"],
+               "energy": other["energy"], "acceptance": other["acceptance"]}
+        if other_prec == 32:
+            rec["refresh"] = {"sweeps": args.refresh, "guard": args.guard, **other["drift"]}
+        out["mixed_path" if other_prec == 32 else "fp64_path"] = rec
+        mixed_ms, fp64_ms = (other["ms"], main_rec["ms"]) if other_prec == 32 else (main_rec["ms"], other["ms"])
+        out["mixed_over_fp64"] = {"sweeps": fp64_ms / mixed_ms, "sr_step": fp64_ms / mixed_ms}
+        out["accuracy"] = acc
+        if acc:
+            out["accuracy"]["dE_per_site"] = acc["dE"] / ns
+    if os.environ.get("MVMC_B200_TIMERS") == "1":
+        out["timers"] = "phase cycles: run the engine directly for mvmc_b200_sampler_timers"
+    print(json.dumps(out), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------------------
+# Pfaffian workloads.
+# ----------------------------------------------------------------------------------------
+def fp64_gemm_peak():
+    """cuBLAS FP64 GEMM throughput (TFLOP/s) on this GPU, best of 5: the FP64 denominator."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / (best / 1e3) / 1e12
+
+
+def reference_pfinv(args):
+    sizes = PFINV[args.config]
+    procs = os.cpu_count() or 1
+    per = 1024 if len(set(sizes)) == 1 else 128
+    planes = procs * per * len(set(sizes))
+    pool = CpuPool(procs, initializer=_pfinv_init, initargs=(sizes, per))
+    for _ in range(args.warmup):
+        pool.time(_pfinv_job, range(procs))
+    times = [pool.time(_pfinv_job, range(procs)) for _ in range(args.steps)]
+    pool.close()
+    t = sum(times) / len(times)
+    value = planes / t
+    return {"metric": PFINV_METRIC, "value": value, "unit": "planes/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config, "sizes": sorted(set(sizes))},
+            "cpu_baseline": {"value": value, "unit": "planes/s", "cores": procs, "kind": "port",
+                             "sample": f"{per} planes of each size per process, one process per core"},
+            "e2e": {"value": value, "unit": "planes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def pfinv_bench(args, ws, rank, local):
+    import ctypes
+    import torch
+    import mvmc_b200 as mb
+    torch.cuda.set_device(local)
+    sizes = PFINV[args.config]
+    B = len(sizes)
+    rng = np.random.default_rng(2024 + rank)
+    uniq = sorted(set(sizes))
+    planes_by_n = {n: skew_planes(rng, n, sizes.count(n)) for n in uniq}
+    cursor = {n: 0 for n in uniq}
+    chunks = []
+    for n in sizes:
+        chunks.append(planes_by_n[n][cursor[n]].ravel())
+        cursor[n] += 1
+    x_host = np.concatenate(chunks)
+    sizes_host = np.asarray(sizes, dtype=np.int32)
+    offsets_host = np.concatenate([[0], np.cumsum(sizes_host.astype(np.int64) ** 2)[:-1]]).astype(np.int64)
+    n_max = max(sizes)
+    uniform = len(uniq) == 1
+    dev = torch.device("cuda", local)
+    x = torch.from_numpy(x_host).to(dev)
+    inv = torch.empty_like(x)
+    pf = torch.zeros(B, dtype=torch.float64, device=dev)
+    st = torch.zeros(B, dtype=torch.int32, device=dev)
+    sz = torch.from_numpy(sizes_host).to(dev)
+    off = torch.from_numpy(offsets_host).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    L = mb.lib()
+
+    def launch():
+        rc = L.mvmc_b200_pfinv_batch_device(P(x), None if uniform else P(sz), None if uniform else P(off),
+                                            n_max if uniform else 0, B, n_max, P(pf), P(inv), P(st),
+                                            args.precision, ctypes.c_void_p(stream.cuda_stream))
+        if rc < 0:
+            raise RuntimeError(L.mvmc_b200_last_error().decode())
+
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    if int((st != 0).sum()) != 0:
+        raise RuntimeError("singular planes in the Pfaffian workload")
+    clocks_path = os.path.join(tempfile.mkdtemp(prefix="mvmc_pf_"), "clocks.csv")
+    sampler = start_clock_sampler(clocks_path) if rank == 0 else None
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
+        launch()
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    stop_clock_sampler(sampler)
+    per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms = sum(per) / len(per)
+    # end to end through the host-buffer entry points (allocation + copies in the region)
+    pf_h = np.zeros(B)
+    inv_h = np.zeros_like(x_host)
+    st_h = np.zeros(B, dtype=np.int32)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        if uniform:
+            rc = L.mvmc_b200_pfinv_batch(vp(x_host), n_max, B, vp(pf_h), vp(inv_h), vp(st_h))
+        else:
+            rc = L.mvmc_b200_pfinv_batch_mixed(vp(x_host), vp(sizes_host), B, args.precision, vp(pf_h),
+                                               vp(inv_h), vp(st_h))
+        if rc < 0:
+            raise RuntimeError(L.mvmc_b200_last_error().decode())
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    flops = float(sum(2 * n ** 3 for n in sizes))
+    bytes_ = float(sum(16 * n * n for n in sizes))
+    peak_tf = fp64_gemm_peak()
+    achieved = flops / (ms / 1e3) / 1e12
+    hbm, hbm_kind = measured_peaks()
+    base_planes = 256 if uniform else 32
+    base_t = cpu_pfinv_time(sizes, base_planes)
+    base_value = base_planes * len(uniq) / base_t
+    out = {
+        "metric": PFINV_METRIC, "value": ws * B / (ms / 1e3), "unit": "planes/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == 64 else "f32sweep",
+        "data": "synthetic",
+        "config": {"workload": args.config, "planes": B, "sizes": uniq, "precision": args.precision,
+                   "l2": "inputs larger than L2 (x + inverse > 126 MB)"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": achieved / peak_tf, "traffic": None, "kernel": "k_pfinv_pp/k_pfinv_batch",
+                     "peak_kind": "cuBLAS FP64 GEMM measured in this run",
+                     "hbm_gbs": bytes_ / (ms / 1e3) / 1e9, "hbm_peak": hbm, "hbm_peak_kind": hbm_kind},
+        "cpu_baseline": {"value": base_value, "unit": "planes/s", "cores": 1, "kind": "port",
+                         "sample": f"{base_planes} planes of each size {uniq}"},
+        "e2e": {"value": ws * B / e2e_s, "unit": "planes/s", "h2d_bytes_per_step": int(x_host.nbytes + 4 * B),
+                "d2h_bytes_per_step": int(inv_h.nbytes + 8 * B + 4 * B)},
+        "gpu_launches": args.steps,
+        "clocks": summarize_clocks(clocks_path, local),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
 
 
 def main():
@@ -106,154 +545,31 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="square8")
-    ap.add_argument("--precision", type=int, default=64)
+    ap.add_argument("--config", default="square8", choices=sorted(WALKERS) + sorted(PFINV))
+    ap.add_argument("--precision", type=int, default=64, choices=(32, 64),
+                    help="64: plain FP64 path (default); 32: mixed path (FP32 inverses, FP64 refresh)")
     ap.add_argument("--walkers", type=int, default=0)
+    ap.add_argument("--interval", type=int, default=0, help="override NVMCInterval (sweeps per sample block)")
     ap.add_argument("--refresh", type=int, default=32,
                     help="mixed path: FP64 refresh every this many sweeps (0: the C accept-window rule)")
+    ap.add_argument("--guard", type=float, default=0.03,
+                    help="mixed path: FP64 refresh after an accepted move with a plane ratio outside [g, 1/g]")
+    ap.add_argument("--no-compare", action="store_true", help="time one path only (no other precision beside it)")
+    ap.add_argument("--sr-precision", type=int, default=0, choices=(0, 64, 32, 16),
+                    help="SR operator storage of the timed engine (0: FP64)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     ws, rank, local = dist_env()
-
-    import lattice
-    cfg = dict(lattice.CONFIGS[args.config])
-    W = args.walkers or WALKERS[args.config]
-    tmp = tempfile.mkdtemp(prefix=f"mvmc_bench_{rank}_")
-    namelist, initial_def, dims = lattice.write_inputs(os.path.join(tmp, "in"), **cfg)
-    S = cfg["samples"]
-    sweeps_per_walker_step = (S + 1) * cfg["interval"]  # burn-in chain: NVMCSample + 1 blocks
-
+    pf = args.config in PFINV
     if args.impl == "reference":
         if rank != 0:
             return
-        procs = os.cpu_count() or 1
-        per = max(1, 2 if args.config != "chain16" else 64)
-        # the oracle's first step includes warm-up blocks: (warmup + S) blocks per walker
-        sweeps = procs * per * (cfg["warmup"] + S) * cfg["interval"]
-        times = []
-        for _ in range(args.warmup):
-            cpu_baseline(namelist, initial_def, per, procs)
-        for _ in range(args.steps):
-            times.append(cpu_baseline(namelist, initial_def, per, procs))
-        t = sum(times) / len(times)
-        value = sweeps / t
-        line = {"metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "impl": "reference",
-                "config": {"workload": args.config, "walkers": procs * per, "sweeps_per_walker": (cfg["warmup"] + S) * cfg["interval"]},
-                "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": procs, "kind": "port",
-                                 "sample": f"{procs * per} chains x one SR step (warm-up + {S} sample blocks) of {args.config}"},
-                "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(reference_pfinv(args) if pf else reference_engine(args)), flush=True)
         return
-
-    import torch
-    import mvmc_b200 as mb
-    if ws > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", init_method="env://",
-                                timeout=__import__("datetime").timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    eng = mb.Engine(namelist, initial_def, walkers=W, precision=args.precision, seed=12345 + rank * W,
-                    device=local, refresh_sweeps=args.refresh if args.precision == 32 else 0)
-    stream = torch.cuda.ExternalStream(eng.stream())
-    info = {}
-
-    def sr_step():
-        eng.sample()
-        e, ho, oo = eng.measure()
-        rc, sri = eng.sr_cg()
-        info["energy"] = float(e[1])
-        info["cg_info"] = int(sri[8])
-        return e
-
-    for _ in range(args.warmup):
-        sr_step()
-    torch.cuda.synchronize()
-    clocks_path = os.path.join(tmp, "clocks.csv")
-    sampler = start_clock_sampler(clocks_path) if rank == 0 else None
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    samp_ms = []
-    h0, d0 = eng.transfer_bytes()
-    t_wall0 = time.perf_counter()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        eng.sample()
-        b.record(stream)
-        e, ho, oo = eng.measure()
-        rc, sri = eng.sr_cg()
-        info["energy"] = float(e[1])
-        samp_ms.append((a, b))
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t_wall = time.perf_counter() - t_wall0
-    h1, d1 = eng.transfer_bytes()
-    if sampler is not None:
-        sampler.terminate()
-        sampler.wait()
-    ms = ev0.elapsed_time(ev1)
-    samp = [a.elapsed_time(b) for a, b in samp_ms]
-    if ws > 1:
-        t = torch.tensor([ms, t_wall * 1e3], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, t_wall_ms = float(t[0]), float(t[1])
+    if pf:
+        pfinv_bench(args, ws, rank, local)
     else:
-        t_wall_ms = t_wall * 1e3
-    sweeps_total = ws * W * sweeps_per_walker_step * args.steps
-    value = sweeps_total / (ms / 1e3)
-    samples = eng.samples()
-    c = samples["counter"].reshape(-1, 6).sum(axis=0)
-    proposals = int(c[0] + c[2])
-    p_acc = (c[1] + c[3]) / max(1, proposals)
-    n, nqp, ns = dims["n"], dims["nqp"], dims["nsite"]
-    s_bytes = 8 if args.precision == 64 else 4
-    # algorithmic bytes per walker-sweep of the resident sampler (row reads per proposal,
-    # rank-2 read+write per accepted move)
-    per_sweep = ns * (nqp * n * s_bytes + nqp * n * 8) + ns * p_acc * nqp * (2 * n * n * s_bytes)
-    launch_bytes = W * sweeps_per_walker_step * per_sweep
-    samp_avg_ms = sum(samp) / len(samp)
-    achieved = launch_bytes / (samp_avg_ms / 1e3) / 1e9
-    peak, peak_kind = measured_peaks()
-    out = None
-    if rank == 0:
-        base_t = cpu_baseline(namelist, initial_def, 1, 1)
-        base_sweeps = (cfg["warmup"] + S) * cfg["interval"]
-        clocks = summarize_clocks(clocks_path, local)
-        out = {
-            "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == 64 else "f32+f64refresh",
-            "data": "synthetic",
-            "config": {"workload": args.config, "walkers_per_gpu": W, "nsite": ns, "n": n, "nqp": nqp,
-                       "npara": dims["npara"], "sweeps_per_walker_step": sweeps_per_walker_step,
-                       "precision": args.precision, "parallelism": f"replicas{ws}",
-                       "refresh_sweeps": args.refresh if args.precision == 32 else None,
-                       "l2": "inputs larger than L2 between steps (walker planes + O matrix)"},
-            "sr_step_ms": ms / args.steps, "sample_ms": samp_avg_ms, "energy": info.get("energy"),
-            "acceptance": p_acc,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_sample",
-                         "peak_kind": peak_kind},
-            "cpu_baseline": {"value": base_sweeps / base_t, "unit": "sweeps/s", "cores": 1, "kind": "port",
-                             "sample": f"1 chain x one SR step (warm-up + {S} blocks, {base_sweeps} sweeps) of {args.config}"},
-            "e2e": {"value": sweeps_total / (t_wall_ms / 1e3), "unit": "sweeps/s",
-                    "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps},
-            "gpu_launches": 8 * args.steps,
-            "residency": os.environ.get("MVMC_B200_RESIDENCY", "auto"),
-            "phase_cycles_per_walker": ({k: v / W for k, v in eng.sampler_timers().items()}
-                                        if os.environ.get("MVMC_B200_TIMERS") == "1" else None),
-            "clocks": clocks,
-        }
-        print(json.dumps(out), flush=True)
-    eng.close()
-    if ws > 1:
-        dist.destroy_process_group()
+        engine_bench(args, ws, rank, local)
 
 
 if __name__ == "__main__":

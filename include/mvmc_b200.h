@@ -62,6 +62,10 @@ typedef struct mvmc_b200_options {
   int saved_per_walker; /* samples saved per walker and SR step; 0 = NVMCSample (C semantics) */
   long long seed;       /* < 0: RndSeed of modpara.def */
   int device;           /* CUDA device ordinal */
+  int sr_precision;     /* SR-CG sample matrix: 64 (or 0) FP64 in the C order; 32 FP32 or 16 BF16,
+                         * centred and column-scaled, FP32 products (the mixed path's operator) */
+  double refresh_guard; /* g in [0, 1): FP64 refresh right after an accepted move whose Pfaffian
+                         * ratio on any QP plane lies outside [g, 1/g]; 0 = off (C behaviour) */
 } mvmc_b200_options;
 
 void mvmc_b200_default_options(mvmc_b200_options* opt);
@@ -107,6 +111,11 @@ int mvmc_b200_measure(mvmc_b200_ctx* ctx, double* energy, double* ho, double* oo
 int mvmc_b200_get_o_store(const mvmc_b200_ctx* ctx, double* o_store, long long count);
 /* Per-sample local energies (W*S). */
 int mvmc_b200_get_local_energies(const mvmc_b200_ctx* ctx, double* e_loc, long long count);
+/* Per-sample ln|Psi(x)| (W*S) of the last measurement: the Gutzwiller-Jastrow exponent
+ * sum_k alpha_k c_k plus ln|IP| (calculate_ip_real, observables.rs:128; log_proj_ratio,
+ * projection.rs:403). With set_parameters + measure on the same saved samples this gives
+ * ln|Psi| at shifted parameters, the finite-difference check of the O rows. */
+int mvmc_b200_get_log_amplitudes(const mvmc_b200_ctx* ctx, double* log_psi, long long count);
 
 /* SR-CG step: stochastic_opt_cg_with_reducer (sr_cg.rs:201-490) with
  * SampledSrOperator::solve_with_product (sr_cg.rs:700-880) run on the device; S·v is
@@ -160,6 +169,47 @@ int mvmc_b200_run_opt(const char* namelist, const char* initial_def, const char*
  * for the last mvmc_b200_sample, measured by each walker's control thread. Zero unless the
  * environment variable MVMC_B200_TIMERS=1 was set when the context was created. */
 int mvmc_b200_sampler_timers(const mvmc_b200_ctx* ctx, double* cycles);
+
+/* Accuracy of the incrementally updated amplitudes in the last mvmc_b200_sample. At every
+ * FP64 refresh the drift |ln|IP|_refreshed − ln|IP|_tracked| is recorded; stats[4] =
+ * {max over walkers of each walker's largest drift, mean of those, scheduled refreshes
+ * per walker (C rule or refresh_sweeps), guard-triggered refreshes per walker}. */
+int mvmc_b200_refresh_stats(const mvmc_b200_ctx* ctx, double* stats);
+
+/* ---------------------------------------------------------------------------------
+ * One walker's Pfaffian stage: the five operations of RealPfStage
+ * (crates/mvmc-core/src/sampling/stage.rs:56-129) on device-resident FP64 inverses, for a
+ * host-driven (teacher-forced) chain. The host keeps the configuration and the RNG and
+ * passes the candidate configuration ele_idx[2*Ne] (sites, the move already applied) with
+ * every call; the stage reads the context's Slater table (set_parameters rebuilds it).
+ * Slots: electron ma of spin sa is slot ma + sa*Ne. Pfaffian vectors have NQP entries.
+ * ------------------------------------------------------------------------------- */
+typedef struct mvmc_b200_stage mvmc_b200_stage;
+
+int mvmc_b200_stage_create(mvmc_b200_ctx* ctx, mvmc_b200_stage** out);
+void mvmc_b200_stage_destroy(mvmc_b200_stage* stage);
+/* begin (stage.rs:60): build the resident inverses of ele_idx; pf may be NULL. */
+int mvmc_b200_stage_begin(mvmc_b200_stage* stage, const int64_t* ele_idx, double* pf);
+/* propose_hop (stage.rs:71-81): pf_new[q] of the one-electron move of slot (ma, spin). */
+int mvmc_b200_stage_propose_hop(mvmc_b200_stage* stage, const int64_t* ele_idx, int ma, int spin,
+                                double* pf_new);
+/* accept_hop (stage.rs:83-92): rank-2 inverse update; the current Pf become pf_new
+ * (NULL keeps the update's own product). */
+int mvmc_b200_stage_accept_hop(mvmc_b200_stage* stage, const int64_t* ele_idx, int ma, int spin,
+                               const double* pf_new);
+/* propose_exchange (stage.rs:94-102): pf_new of the two-electron exchange of slots
+ * (ma, sa) and (mb, sb). */
+int mvmc_b200_stage_propose_exchange(mvmc_b200_stage* stage, const int64_t* ele_idx, int ma, int sa,
+                                     int mb, int sb, double* pf_new);
+/* accept_exchange (stage.rs:104-114): rank-4 update; ra_old, rb_old are the sites before
+ * the move. */
+int mvmc_b200_stage_accept_exchange(mvmc_b200_stage* stage, const int64_t* ele_idx, int ma, int sa,
+                                    int mb, int sb, int ra_old, int rb_old);
+/* recompute (stage.rs:116-123): returns 1 on a numeric failure (zero pivot), 0 ok. */
+int mvmc_b200_stage_recompute(mvmc_b200_stage* stage, const int64_t* ele_idx, double* pf);
+/* Current Pf[NQP] and inverses inv_m[NQP][n*n] in mVMC's InvM layout (column-major -X^-1,
+ * state.rs:208, without the pad slot); either may be NULL. */
+int mvmc_b200_stage_state(const mvmc_b200_stage* stage, double* pf, double* inv_m);
 
 /* The context's CUDA stream (a cudaStream_t), for timing and ordering with caller work. */
 void* mvmc_b200_stream(mvmc_b200_ctx* ctx);

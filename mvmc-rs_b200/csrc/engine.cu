@@ -23,13 +23,20 @@ int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStr
 bool sample_planes_in_smem(const DevModel& m, int precision, int limit);
 int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                   double* eloc, int* valid, unsigned* status, cudaStream_t stream);
+                   double* eloc, double* lpsi, int* valid, unsigned* status, cudaStream_t stream);
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,
                   const int* valid, const int* s_num, double* wsum, double* tot, cudaStream_t stream);
 int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
                          double* oa, cudaStream_t stream);
 int launch_sr_cg(CgArgs a, cudaStream_t stream);
 int cg_grid_blocks(long long ns, int na);
+int low_lda(int na, int kind);
+int cg_grid_blocks_kind(long long ns, int na, int kind);
+int cg_nchunk(long long ns, int na, int kind, int blocks);
+int launch_gather_active_low(const double* store, int sr_size, long long ns, const int* map, int na,
+                             const double* mean, const double* cs, int kind, void* out, cudaStream_t stream);
+int launch_stage(const DevModel& m, const StageBufs& b, int op, int msa, int msb, int rsa_old, int rsb_old,
+                 unsigned* status, cudaStream_t stream);
 
 // K0: SlaterElm[q][rs_i][rs_j] from the Slater parameters (update_slater_elm,
 // crates/mvmc-core/src/slater_update.rs:17-120).
@@ -92,6 +99,7 @@ struct mvmc_b200_ctx {
   float* d_slater32 = nullptr;
   double* d_ostore = nullptr;
   double* d_eloc = nullptr;
+  double* d_lpsi = nullptr;
   int* d_valid = nullptr;
   double* d_wsum = nullptr;
   double* d_tot = nullptr;
@@ -99,7 +107,8 @@ struct mvmc_b200_ctx {
   int gws_blocks = 0;
   // SR-CG buffers
   double* d_oa = nullptr;
-  size_t oa_cap = 0;
+  size_t oa_cap = 0;  // doubles
+  size_t y_cap = 0;
   double* d_cgvec = nullptr;  // mean, diag, g, x, r, d, q
   size_t cgvec_cap = 0;
   double* d_y = nullptr;
@@ -185,6 +194,10 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   c->W = std::max(1, opt.walkers);
   c->S = opt.saved_per_walker > 0 ? opt.saved_per_walker : m.nvmc_sample;
   if (opt.precision != 64 && opt.precision != 32) throw std::runtime_error("precision must be 64 or 32");
+  if (opt.sr_precision != 0 && opt.sr_precision != 64 && opt.sr_precision != 32 && opt.sr_precision != 16)
+    throw std::runtime_error("sr_precision must be 0, 64, 32 or 16");
+  if (!(opt.refresh_guard >= 0.0 && opt.refresh_guard < 1.0))
+    throw std::runtime_error("refresh_guard must lie in [0, 1)");
   // walker streams: seed RndSeed + w, each consuming init_parameter draws (multichain.rs:88)
   const long long base = opt.seed >= 0 ? opt.seed : m.rnd_seed;
   std::vector<uint32_t> sf(static_cast<size_t>(c->W) * kSfmtN32);
@@ -292,6 +305,11 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   dw.status = c->alloc<unsigned>(1);
   check(cudaMemset(dw.status, 0, sizeof(unsigned)), "memset status");
   dw.refresh_sweeps = opt.refresh_sweeps;
+  dw.drift = c->alloc<double>(W);
+  check(cudaMemset(dw.drift, 0, sizeof(double) * W), "memset drift");
+  dw.nrefresh = c->alloc<long long>(2 * static_cast<size_t>(W));
+  check(cudaMemset(dw.nrefresh, 0, sizeof(long long) * 2 * W), "memset refresh counts");
+  dw.refresh_guard = opt.refresh_guard;
   dw.timers = nullptr;
   if (const char* t = std::getenv("MVMC_B200_TIMERS")) {
     if (std::strcmp(t, "1") == 0) {
@@ -317,6 +335,7 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   const size_t rows = static_cast<size_t>(W) * S;
   c->d_ostore = c->alloc<double>(rows * dm.sr_size);
   c->d_eloc = c->alloc<double>(rows);
+  c->d_lpsi = c->alloc<double>(rows);
   c->d_valid = c->alloc<int>(rows);
   c->d_wsum = c->alloc<double>(static_cast<size_t>(W) * (5 + 3 * dm.sr_size));
   c->d_tot = c->alloc<double>(5 + 3 * dm.sr_size);
@@ -331,6 +350,9 @@ template <typename F>
 int guarded(F&& f) {
   try {
     return f();
+  } catch (const std::invalid_argument& e) {
+    mvmcb::set_last_error(e.what());
+    return MVMC_B200_EARG;
   } catch (const std::exception& e) {
     mvmcb::set_last_error(e.what());
     const std::string what = e.what();
@@ -342,7 +364,7 @@ int guarded(F&& f) {
 int do_measure(mvmc_b200_ctx* c) {
   const int rows = c->W * c->S;
   int rc = launch_measure(c->dm, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, rows, c->d_gws,
-                          c->gws_blocks, c->d_ostore, c->d_eloc, c->d_valid, c->dw.status, c->stream);
+                          c->gws_blocks, c->d_ostore, c->d_eloc, c->d_lpsi, c->d_valid, c->dw.status, c->stream);
   if (rc != kOk) return rc;
   rc = launch_reduce(c->dm, c->W, c->S, c->d_ostore, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
                      c->stream);
@@ -398,30 +420,49 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
     vecs[2 * na + si] = -dt * (ho[idx] - ho[0] * mean_all[idx]);
   }
   const long long ns = static_cast<long long>(c->W) * c->S;
-  if (static_cast<size_t>(ns) * na > c->oa_cap) {
-    c->d_oa = c->alloc<double>(static_cast<size_t>(ns) * na);
-    c->oa_cap = static_cast<size_t>(ns) * na;
-    c->d_y = c->alloc<double>(ns);
+  // operator storage: 0 FP64 (C order), 1 FP32, 2 BF16 (centred, column-scaled)
+  const int kind = c->opt.sr_precision == 32 ? 1 : (c->opt.sr_precision == 16 ? 2 : 0);
+  const size_t oa_need = kind == 0 ? static_cast<size_t>(ns) * na
+                                   : (static_cast<size_t>(ns) * low_lda(na, kind) * (kind == 1 ? 4 : 2) + 7) / 8;
+  if (oa_need > c->oa_cap) {
+    c->d_oa = c->alloc<double>(oa_need);
+    c->oa_cap = oa_need;
   }
-  if (static_cast<size_t>(7) * na > c->cgvec_cap) {
-    c->d_cgvec = c->alloc<double>(static_cast<size_t>(7) * na);
-    c->cgvec_cap = static_cast<size_t>(7) * na;
+  if (static_cast<size_t>(ns) > c->y_cap) {
+    c->d_y = c->alloc<double>(ns);
+    c->y_cap = static_cast<size_t>(ns);
+  }
+  if (static_cast<size_t>(8) * na > c->cgvec_cap) {
+    c->d_cgvec = c->alloc<double>(static_cast<size_t>(8) * na);
+    c->cgvec_cap = static_cast<size_t>(8) * na;
   }
   if (static_cast<size_t>(na) > c->map_cap) {
     c->d_map = c->alloc<int>(na);
     c->map_cap = na;
   }
-  const int blocks = cg_grid_blocks(ns, na);
-  const int ntile = (na + 255) / 256;
-  const int nchunk = static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, blocks / ntile))));
+  const int blocks = cg_grid_blocks_kind(ns, na, kind);
+  const int nchunk = cg_nchunk(ns, na, kind, blocks);
   if (static_cast<size_t>(nchunk) * na > c->part_cap) {
     c->d_part = c->alloc<double>(static_cast<size_t>(nchunk) * na);
     c->part_cap = static_cast<size_t>(nchunk) * na;
   }
   check(cudaMemcpyAsync(c->d_map, map.data(), sizeof(int) * na, cudaMemcpyHostToDevice, c->stream), "upload map");
+  if (kind != 0) {
+    // column scales: the standard deviation of each active column (1 where it vanishes)
+    vecs.resize(static_cast<size_t>(8) * na);
+    for (int si = 0; si < na; ++si) {
+      const double v = vecs[na + si];
+      vecs[7 * static_cast<size_t>(na) + si] = (std::isfinite(v) && v > 0.0) ? std::sqrt(v) : 1.0;
+    }
+    check(cudaMemcpyAsync(c->d_cgvec + 7 * static_cast<size_t>(na), vecs.data() + 7 * static_cast<size_t>(na),
+                          sizeof(double) * na, cudaMemcpyHostToDevice, c->stream), "upload column scales");
+    c->h2d += static_cast<long long>(sizeof(double) * na);
+  }
   check(cudaMemcpyAsync(c->d_cgvec, vecs.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, c->stream),
         "upload cg vectors");
-  int rc = launch_gather_active(c->d_ostore, size, ns, c->d_map, na, c->d_oa, c->stream);
+  int rc = kind == 0 ? launch_gather_active(c->d_ostore, size, ns, c->d_map, na, c->d_oa, c->stream)
+                     : launch_gather_active_low(c->d_ostore, size, ns, c->d_map, na, c->d_cgvec,
+                                                c->d_cgvec + 7 * static_cast<size_t>(na), kind, c->d_oa, c->stream);
   if (rc != kOk) return rc;
   CgArgs a;
   a.O = c->d_oa;
@@ -444,6 +485,12 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   a.inv_w = 1.0 / wc;
   a.shift = m.sta_del;
   a.tol = m.cg_tol;
+  if (kind != 0) {
+    a.Ol = c->d_oa;
+    a.cs = c->d_cgvec + 7 * static_cast<size_t>(na);
+    a.lda = low_lda(na, kind);
+    a.o_kind = kind;
+  }
   rc = launch_sr_cg(a, c->stream);
   if (rc != kOk) return rc;
   std::vector<double> x(na), scal(8);
@@ -604,6 +651,17 @@ extern "C" int mvmc_b200_get_o_store(const mvmc_b200_ctx* c, double* o_store, lo
   });
 }
 
+extern "C" int mvmc_b200_get_log_amplitudes(const mvmc_b200_ctx* c, double* log_psi, long long count) {
+  if (!c || !log_psi) return MVMC_B200_EARG;
+  const long long need = static_cast<long long>(c->W) * c->S;
+  if (count < need) return MVMC_B200_EARG;
+  if (!c->measured) return MVMC_B200_ESTATE;
+  return guarded([&]() {
+    check(cudaMemcpy(log_psi, c->d_lpsi, sizeof(double) * need, cudaMemcpyDeviceToHost), "download ln|psi|");
+    return MVMC_B200_OK;
+  });
+}
+
 extern "C" int mvmc_b200_get_local_energies(const mvmc_b200_ctx* c, double* e_loc, long long count) {
   if (!c || !e_loc) return MVMC_B200_EARG;
   const long long need = static_cast<long long>(c->W) * c->S;
@@ -628,6 +686,28 @@ extern "C" int mvmc_b200_sampler_timers(const mvmc_b200_ctx* c, double* cycles) 
     check(cudaMemcpy(t.data(), c->dw.timers, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost), "timers");
     for (int w = 0; w < c->W; ++w)
       for (int k = 0; k < kPhCount; ++k) cycles[k] += static_cast<double>(t[static_cast<size_t>(w) * kPhCount + k]);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_refresh_stats(const mvmc_b200_ctx* c, double* stats) {
+  if (!c || !stats) return MVMC_B200_EARG;
+  return guarded([&]() {
+    std::vector<double> d(c->W);
+    std::vector<long long> r(2 * static_cast<size_t>(c->W));
+    check(cudaMemcpy(d.data(), c->dw.drift, sizeof(double) * c->W, cudaMemcpyDeviceToHost), "drift");
+    check(cudaMemcpy(r.data(), c->dw.nrefresh, sizeof(long long) * r.size(), cudaMemcpyDeviceToHost), "refreshes");
+    double mx = 0.0, sum = 0.0, sched = 0.0, guard = 0.0;
+    for (int w = 0; w < c->W; ++w) {
+      mx = std::max(mx, d[w]);
+      sum += d[w];
+      sched += static_cast<double>(r[2 * static_cast<size_t>(w)]);
+      guard += static_cast<double>(r[2 * static_cast<size_t>(w) + 1]);
+    }
+    stats[0] = mx;
+    stats[1] = sum / c->W;
+    stats[2] = sched / c->W;
+    stats[3] = guard / c->W;
     return MVMC_B200_OK;
   });
 }
@@ -689,4 +769,180 @@ extern "C" int mvmc_b200_run_opt(const char* namelist, const char* initial_def, 
   });
   mvmc_b200_destroy(c);
   return rc;
+}
+
+// ---------------------------------------------------------------------------------------
+// One walker's Pfaffian stage (RealPfStage, crates/mvmc-core/src/sampling/stage.rs:56-129).
+// ---------------------------------------------------------------------------------------
+struct mvmc_b200_stage {
+  mvmc_b200_ctx* ctx = nullptr;
+  StageBufs b{};
+  int* d_idx = nullptr;
+  std::vector<void*> allocs;
+  ~mvmc_b200_stage() {
+    for (void* p : allocs) cudaFree(p);
+  }
+  template <typename T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    check(cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T)), "stage cudaMalloc");
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
+};
+
+namespace {
+
+// Candidate configuration of the call: validated on the host, copied to the device.
+void stage_upload_idx(mvmc_b200_stage* st, const int64_t* ele_idx) {
+  const mvmc_b200_ctx* c = st->ctx;
+  const int n = c->dm.n;
+  std::vector<int> idx(n);
+  for (int k = 0; k < n; ++k) {
+    if (ele_idx[k] < 0 || ele_idx[k] >= c->dm.ns) throw std::invalid_argument("stage: ele_idx entry out of range");
+    idx[k] = static_cast<int>(ele_idx[k]);
+  }
+  check(cudaMemcpyAsync(st->d_idx, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream), "stage idx");
+}
+
+int stage_run(mvmc_b200_stage* st, int op, int msa, int msb, int rsa_old, int rsb_old) {
+  mvmc_b200_ctx* c = st->ctx;
+  const int rc = launch_stage(c->dm, st->b, op, msa, msb, rsa_old, rsb_old, c->dw.status, c->stream);
+  if (rc != kOk) return rc;
+  return kOk;
+}
+
+void stage_download(mvmc_b200_stage* st, const double* dev, double* host) {
+  mvmc_b200_ctx* c = st->ctx;
+  if (host)
+    check(cudaMemcpyAsync(host, dev, sizeof(double) * c->dm.nqp, cudaMemcpyDeviceToHost, c->stream), "stage pf");
+  check(cudaStreamSynchronize(c->stream), "stage");
+}
+
+int stage_guard(mvmc_b200_stage* st, const int64_t* ele_idx, int ma, int sa, int mb, int sb, bool two) {
+  if (!st || !ele_idx) return MVMC_B200_EARG;
+  const int ne = st->ctx->dm.ne;
+  if (ma < 0 || ma >= ne || sa < 0 || sa > 1) return MVMC_B200_EARG;
+  if (two && (mb < 0 || mb >= ne || sb < 0 || sb > 1 || (ma + sa * ne) == (mb + sb * ne))) return MVMC_B200_EARG;
+  return MVMC_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int mvmc_b200_stage_create(mvmc_b200_ctx* c, mvmc_b200_stage** out) {
+  if (!c || !out) return MVMC_B200_EARG;
+  *out = nullptr;
+  auto* st = new mvmc_b200_stage();
+  st->ctx = c;
+  const int rc = guarded([&]() {
+    const size_t nn = static_cast<size_t>(c->dm.n) * c->dm.n;
+    st->b.planes = st->alloc<double>(nn * c->dm.nqp);
+    st->b.ws = st->alloc<double>(2 * nn);
+    st->b.pf = st->alloc<double>(c->dm.nqp);
+    st->b.pfn = st->alloc<double>(c->dm.nqp);
+    st->d_idx = st->alloc<int>(c->dm.n);
+    st->b.idx = st->d_idx;
+    st->b.info = st->alloc<int>(1);
+    check(cudaMemsetAsync(st->b.pf, 0, sizeof(double) * c->dm.nqp, c->stream), "stage memset");
+    check(cudaMemsetAsync(st->b.pfn, 0, sizeof(double) * c->dm.nqp, c->stream), "stage memset");
+    check(cudaStreamSynchronize(c->stream), "stage create");
+    return MVMC_B200_OK;
+  });
+  if (rc != MVMC_B200_OK) {
+    delete st;
+    return rc;
+  }
+  *out = st;
+  return MVMC_B200_OK;
+}
+
+extern "C" void mvmc_b200_stage_destroy(mvmc_b200_stage* st) { delete st; }
+
+extern "C" int mvmc_b200_stage_recompute(mvmc_b200_stage* st, const int64_t* ele_idx, double* pf) {
+  if (!st || !ele_idx) return MVMC_B200_EARG;
+  return guarded([&]() {
+    stage_upload_idx(st, ele_idx);
+    const int rc = stage_run(st, kStageRecompute, 0, 0, 0, 0);
+    if (rc != kOk) return rc;
+    int info = 0;
+    check(cudaMemcpyAsync(&info, st->b.info, sizeof(int), cudaMemcpyDeviceToHost, st->ctx->stream), "stage info");
+    stage_download(st, st->b.pf, pf);
+    return info != 0 ? 1 : MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_stage_begin(mvmc_b200_stage* st, const int64_t* ele_idx, double* pf) {
+  return mvmc_b200_stage_recompute(st, ele_idx, pf);
+}
+
+extern "C" int mvmc_b200_stage_propose_hop(mvmc_b200_stage* st, const int64_t* ele_idx, int ma, int spin,
+                                           double* pf_new) {
+  const int g = stage_guard(st, ele_idx, ma, spin, 0, 0, false);
+  if (g != MVMC_B200_OK) return g;
+  return guarded([&]() {
+    stage_upload_idx(st, ele_idx);
+    const int rc = stage_run(st, kStageProposeHop, ma + spin * st->ctx->dm.ne, 0, 0, 0);
+    if (rc != kOk) return rc;
+    stage_download(st, st->b.pfn, pf_new);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_stage_accept_hop(mvmc_b200_stage* st, const int64_t* ele_idx, int ma, int spin,
+                                          const double* pf_new) {
+  const int g = stage_guard(st, ele_idx, ma, spin, 0, 0, false);
+  if (g != MVMC_B200_OK) return g;
+  return guarded([&]() {
+    stage_upload_idx(st, ele_idx);
+    const int rc = stage_run(st, kStageAcceptHop, ma + spin * st->ctx->dm.ne, 0, 0, 0);
+    if (rc != kOk) return rc;
+    // afterwards the current Pfaffians equal the proposal's (stage.rs:83-92)
+    if (pf_new)
+      check(cudaMemcpyAsync(st->b.pf, pf_new, sizeof(double) * st->ctx->dm.nqp, cudaMemcpyHostToDevice,
+                            st->ctx->stream), "stage pf_new");
+    stage_download(st, st->b.pf, nullptr);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_stage_propose_exchange(mvmc_b200_stage* st, const int64_t* ele_idx, int ma, int sa,
+                                                int mb, int sb, double* pf_new) {
+  const int g = stage_guard(st, ele_idx, ma, sa, mb, sb, true);
+  if (g != MVMC_B200_OK) return g;
+  return guarded([&]() {
+    stage_upload_idx(st, ele_idx);
+    const int ne = st->ctx->dm.ne;
+    const int rc = stage_run(st, kStageProposeExchange, ma + sa * ne, mb + sb * ne, 0, 0);
+    if (rc != kOk) return rc;
+    stage_download(st, st->b.pfn, pf_new);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_stage_accept_exchange(mvmc_b200_stage* st, const int64_t* ele_idx, int ma, int sa,
+                                               int mb, int sb, int ra_old, int rb_old) {
+  const int g = stage_guard(st, ele_idx, ma, sa, mb, sb, true);
+  if (g != MVMC_B200_OK) return g;
+  const int ns = st->ctx->dm.ns;
+  if (ra_old < 0 || ra_old >= ns || rb_old < 0 || rb_old >= ns) return MVMC_B200_EARG;
+  return guarded([&]() {
+    stage_upload_idx(st, ele_idx);
+    const int ne = st->ctx->dm.ne;
+    const int rc = stage_run(st, kStageAcceptExchange, ma + sa * ne, mb + sb * ne, ra_old + sa * ns, rb_old + sb * ns);
+    if (rc != kOk) return rc;
+    stage_download(st, st->b.pf, nullptr);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_stage_state(const mvmc_b200_stage* st, double* pf, double* inv_m) {
+  if (!st) return MVMC_B200_EARG;
+  return guarded([&]() {
+    const mvmc_b200_ctx* c = st->ctx;
+    const size_t nn = static_cast<size_t>(c->dm.n) * c->dm.n;
+    if (pf) check(cudaMemcpy(pf, st->b.pf, sizeof(double) * c->dm.nqp, cudaMemcpyDeviceToHost), "stage pf");
+    if (inv_m)
+      check(cudaMemcpy(inv_m, st->b.planes, sizeof(double) * nn * c->dm.nqp, cudaMemcpyDeviceToHost), "stage inv");
+    return MVMC_B200_OK;
+  });
 }

@@ -60,7 +60,23 @@ struct DevWalkers {
   unsigned* status;           // [1] sticky
   int refresh_sweeps;         // mixed path: extra FP64 refresh cadence in sweeps (0 = off)
   unsigned long long* timers; // [W*8] clock cycles per sampler phase, or null (off)
+  double* drift;              // [W] max |Δ ln|IP|| between the tracked and the refreshed amplitude
+  long long* nrefresh;        // [W*2] scheduled (C rule / NRefresh) and guard-triggered refreshes
+  double refresh_guard;       // refresh after an accepted move with a plane ratio outside [g, 1/g] (0 off)
 };
+
+// One walker's Pfaffian stage buffers (device): FP64 planes and sweep scratch, Pf, the
+// proposal Pf, the candidate configuration and the recomputation status.
+struct StageBufs {
+  double* planes;  // [nqp][n][n] row-major InvM (= X^-1)
+  double* ws;      // [2][n][n]
+  double* pf;      // [nqp]
+  double* pfn;     // [nqp]
+  const int* idx;  // [n]
+  int* info;       // [1]
+};
+enum StageOp { kStageRecompute = 0, kStageProposeHop, kStageAcceptHop, kStageProposeExchange, kStageAcceptExchange };
+constexpr int kStageThreads = 256;
 
 // Sampler phases timed by thread 0 of each walker (cycles, barrier waits included):
 // candidate, ratio, metropolis, update, refresh, total.
@@ -83,6 +99,13 @@ struct CgArgs {
   long long ns;
   int na, nchunk, max_iter, diag_scale;
   double inv_w, shift, tol;
+  // Reduced-precision operator (o_kind 1: FP32, 2: BF16): the centred, column-scaled
+  // active matrix Ol[s][i] = (O[s][i] − ⟨O⟩_i)/cs[i] (zero rows for skipped samples), row
+  // stride lda, so that S·v = Wc⁻¹·cs ⊙ Olᵀ(Ol·(cs ⊙ v)) + shift·diag ⊙ v. o_kind 0 uses O.
+  const void* Ol = nullptr;
+  const double* cs = nullptr;  // [na]
+  int lda = 0;
+  int o_kind = 0;
 };
 
 }  // namespace mvmcb

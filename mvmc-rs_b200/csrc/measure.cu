@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kMeasThreads)
     k_measure(DevModel m, const int* __restrict__ s_idx, const int* __restrict__ s_cfg,
               const int* __restrict__ s_num, const int* __restrict__ s_cnt, int nsamples,
               double* __restrict__ gws, double* __restrict__ ostore, double* __restrict__ eloc,
-              int* __restrict__ valid, unsigned* status) {
+              double* __restrict__ lpsi, int* __restrict__ valid, unsigned* status) {
   extern __shared__ __align__(16) unsigned char smem[];
   const MeasLayout L = meas_layout(m, kSmemPlane);
   int* idx = reinterpret_cast<int*>(smem + L.idx);
@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(kMeasThreads)
       if (tid == 0) {
         valid[sample] = 0;
         eloc[sample] = 0.0;
+        lpsi[sample] = 0.0;
       }
       for (int k = tid; k < m.sr_size; k += nt) ostore[static_cast<size_t>(sample) * m.sr_size + k] = 0.0;
       __syncthreads();
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(kMeasThreads)
       if (tid == 0) {
         valid[sample] = 0;
         eloc[sample] = 0.0;
+        lpsi[sample] = 0.0;
         atomicOr(status, kDevSingular);
       }
       for (int k = tid; k < m.sr_size; k += nt) ostore[static_cast<size_t>(sample) * m.sr_size + k] = 0.0;
@@ -229,6 +231,10 @@ __global__ void __launch_bounds__(kMeasThreads)
       const bool ok = fabs(ip) >= 1.0e-100 && isfinite(e);
       valid[sample] = ok ? 1 : 0;
       eloc[sample] = ok ? e : 0.0;
+      // ln|Ψ(x)| = Σ_k α_k c_k (Gutzwiller-Jastrow exponent) + ln|IP|
+      double lp = 0.0;
+      for (int k = 0; k < m.nproj; ++k) lp += m.proj[k] * static_cast<double>(cnt[k]);
+      lpsi[sample] = ok ? lp + log(fabs(ip)) : 0.0;
       pf[m.nqp] = ip;
       pf[m.nqp + 1] = ok ? 1.0 : 0.0;
     }
@@ -313,20 +319,20 @@ size_t measure_smem(const DevModel& m, bool smem_plane) { return meas_layout(m, 
 template <int JPL>
 int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                        const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                       double* eloc, int* valid, unsigned* status, cudaStream_t stream, int limit) {
+                       double* eloc, double* lpsi, int* valid, unsigned* status, cudaStream_t stream, int limit) {
   const bool smem_plane = meas_layout(m, true).total <= static_cast<size_t>(limit);
   const size_t smem = meas_layout(m, smem_plane).total;
   if (smem > static_cast<size_t>(limit)) return kErrArgument;
   if (smem_plane) {
     auto kernel = k_measure<JPL, true>;
     MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    kernel<<<nsamples, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc,
+    kernel<<<nsamples, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
                                                      valid, status);
   } else {
     auto kernel = k_measure<JPL, false>;
     MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     kernel<<<std::min(nsamples, gws_blocks), kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples,
-                                                                          gws, ostore, eloc, valid, status);
+                                                                          gws, ostore, eloc, lpsi, valid, status);
   }
   MVMCB_CUDA(cudaGetLastError());
   return kOk;
@@ -334,16 +340,16 @@ int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, co
 
 int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                   double* eloc, int* valid, unsigned* status, cudaStream_t stream) {
+                   double* eloc, double* lpsi, int* valid, unsigned* status, cudaStream_t stream) {
   int dev = 0, limit = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int n = m.n;
-  if (n <= 32) return launch_measure_jpl<1>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
-  if (n <= 64) return launch_measure_jpl<2>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
-  if (n <= 128) return launch_measure_jpl<4>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
-  if (n <= 224) return launch_measure_jpl<7>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
-  if (n <= 256) return launch_measure_jpl<8>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, valid, status, stream, limit);
+  if (n <= 32) return launch_measure_jpl<1>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
+  if (n <= 64) return launch_measure_jpl<2>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
+  if (n <= 128) return launch_measure_jpl<4>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
+  if (n <= 224) return launch_measure_jpl<7>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
+  if (n <= 256) return launch_measure_jpl<8>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
   return kErrArgument;
 }
 

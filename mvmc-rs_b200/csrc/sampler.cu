@@ -14,6 +14,7 @@
 // global slice (L2-resident working set).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
@@ -184,7 +185,7 @@ __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigne
     __syncthreads();
     double pfv;
     int st;
-    if (kGlobalSweep) gj_pfinv_pp<double, JPL, 4>(A, B, n, pfv, st);
+    if (kGlobalSweep) gj_pfinv_pp<double, JPL, (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, B, n, pfv, st);
     else gj_pfinv_pp<double, JPL, 1>(A, B, n, pfv, st);
     if (!fp64_planes) {
       T* P = s.planes + static_cast<size_t>(q) * n * n;
@@ -302,7 +303,9 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
       v2c[c] = j < n ? v2[j] : T(0);
     }
     T* P = s.planes + static_cast<size_t>(q) * n * n;
-    constexpr int RB = 4;  // rows per batch: their loads are issued before any store
+    // rows per batch (their loads are issued before any store), fewer for wide rows so
+    // that several walkers fit an SM's register file
+    constexpr int RB = JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1);
     for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
       T x[RB][JPL];
 #pragma unroll
@@ -473,7 +476,7 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
       tc[c2] = j < n ? vt[j] : T(0);
     }
     T* P = s.planes + static_cast<size_t>(q) * n * n;
-    constexpr int RB = 2;  // rows per batch: their loads are issued before any store
+    constexpr int RB = JPL <= 2 ? 2 : 1;  // rows per batch: their loads are issued before any store
     for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
      T xl[RB][JPL];
 #pragma unroll
@@ -556,8 +559,15 @@ __device__ void make_initial_sample_dev(const DevModel& m, SfmtRef& rng, int* id
   make_proj_cnt_serial(m, num, cnt);
 }
 
+// Walkers per SM the register budget is sized for: one when the planes are in shared
+// memory; with planes in L2, enough CTAs for 24 warps per SM.
+template <int NT, bool kSmemPlanes>
+struct SampOccupancy {
+  static constexpr int kBlocks = kSmemPlanes ? 1 : (768 / NT);
+};
+
 template <typename T, int JPL, int NT, bool kSmemPlanes, bool kSmemWs>
-__global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
+__global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks)) k_sample(DevModel m, DevWalkers w) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int wk = blockIdx.x;
   const int tid = threadIdx.x;
@@ -652,6 +662,8 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
   int n_acc_win = 0;
   const int refresh_every = (sizeof(T) == sizeof(float) && w.refresh_sweeps > 0) ? w.refresh_sweeps * max(1, ns) : 0;
   long long since_refresh = 0;
+  double drift_max = 0.0;
+  long long n_sched = 0, n_guard = 0;  // scheduled and guard-triggered refreshes
 
   long long proposal = 0;
   unsigned long long ph[kPhCount] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -784,11 +796,20 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
         if (!isfinite(wgt)) wgt = -1.0;
         const double u = rng.real2();
         const int acc = wgt > u ? 1 : 0;
+        int guard = 0;
         if (acc) {
           for (int k = 0; k < m.nproj; ++k) s.cnt[k] = s.cntn[k];
           s.dctl[dLogIp] = lip_new;
           ++n_acc_win;
           counter[type == 0 ? 1 : 3]++;
+          if (w.refresh_guard > 0.0) {
+            // a plane whose Pfaffian ratio leaves [g, 1/g] passes near a singular matrix:
+            // the rank-2 update amplifies the inverse's rounding error by about 1/|ratio|
+            for (int q = 0; q < m.nqp; ++q) {
+              const double r = fabs(s.pfn[q] / s.pf[q]);
+              if (!(r >= w.refresh_guard && r * w.refresh_guard <= 1.0)) guard = 1;
+            }
+          }
         } else if (type == 0) {
           revert_electron(m, s.idx, s.cfg, s.num, cc[cMi], ri, rj, sp);
         } else {
@@ -804,7 +825,13 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
           refresh = 1;  // C rule: recompute when the accept window exceeds Nsite
           n_acc_win = 0;
         }
+        if (guard && !refresh) refresh = 3;
         if (refresh) since_refresh = 0;
+        if (refresh == 3) {
+          ++n_guard;
+          n_acc_win = 0;
+        }
+        else if (refresh) ++n_sched;
         cc[cRefresh] = refresh;
       }
       __syncthreads();
@@ -819,8 +846,13 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
       lap(kPhUpdate);
       if (cc[cRefresh]) {
         const int info = calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
-        if (tid == 0 && info == 0 && cc[cRefresh] == 1) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
-        if (tid == 0 && info == 0 && cc[cRefresh] == 2) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
+        if (tid == 0 && info == 0) {
+          // drift of the incrementally updated amplitude against the FP64 recomputation
+          const double fresh = log_ip_of(m, s.pf, s.qpw);
+          const double d = fabs(fresh - s.dctl[dLogIp]);
+          if (isfinite(d) && d > drift_max) drift_max = d;
+          s.dctl[dLogIp] = fresh;
+        }
         __syncthreads();
         lap(kPhRefresh);
       }
@@ -850,6 +882,11 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
     w.draws[wk] = sf_draws;
     w.burn[wk] = 1;
     for (int k = 0; k < 6; ++k) w.counter[static_cast<size_t>(wk) * 6 + k] = counter[k];
+    if (w.drift) w.drift[wk] = drift_max;
+    if (w.nrefresh) {
+      w.nrefresh[2 * static_cast<size_t>(wk)] = n_sched;
+      w.nrefresh[2 * static_cast<size_t>(wk) + 1] = n_guard;
+    }
     if (timing) {
       ph[kPhTotal] = clock64() - t_begin;
       for (int k = 0; k < kPhCount; ++k) w.timers[static_cast<size_t>(wk) * kPhCount + k] = ph[k];
@@ -860,9 +897,21 @@ __global__ void __launch_bounds__(NT) k_sample(DevModel m, DevWalkers w) {
 // ---- host launch ---------------------------------------------------------------------------
 int smem_limit_bytes();
 
+int walkers_per_sm();
+
 template <typename T, int JPL, int NT, bool kSmemPlanes, bool kSmemWs>
 int launch_sample_t(const DevModel& m, const DevWalkers& w, cudaStream_t stream) {
-  const size_t smem = samp_layout<T>(m, kSmemPlanes, kSmemWs).total;
+  size_t smem = samp_layout<T>(m, kSmemPlanes, kSmemWs).total;
+  if (!kSmemPlanes && walkers_per_sm() > 0) {
+    // cap the walkers resident per SM (so that their L2 slices stay in L2) by the
+    // shared-memory footprint of each CTA
+    int dev = 0, per_sm = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    const size_t cap = static_cast<size_t>(per_sm / walkers_per_sm() - reserved);
+    smem = std::max(smem, cap);
+  }
   auto kernel = k_sample<T, JPL, NT, kSmemPlanes, kSmemWs>;
   MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   kernel<<<w.W, NT, smem, stream>>>(m, w);
@@ -894,24 +943,50 @@ int residency_policy() {
   return policy;
 }
 
+// Walkers resident per SM when planes are in L2 (MVMC_B200_WPS=k; 0 = as many as fit).
+int walkers_per_sm() {
+  static int k = -1;
+  if (k < 0) {
+    const char* v = std::getenv("MVMC_B200_WPS");
+    k = v ? std::max(0, std::atoi(v)) : 0;
+  }
+  return k;
+}
+
+// CTA size for walkers whose planes are in L2 (MVMC_B200_THREADS=128|256; default 256).
+int global_threads() {
+  static int nt = -1;
+  if (nt < 0) {
+    const char* v = std::getenv("MVMC_B200_THREADS");
+    nt = (v && std::strcmp(v, "128") == 0) ? 128 : 256;
+  }
+  return nt;
+}
+
+template <typename T, int JPL>
+int launch_sample_global(const DevModel& m, const DevWalkers& w, cudaStream_t stream) {
+  if (global_threads() == 128) return launch_sample_t<T, JPL, 128, false, false>(m, w, stream);
+  return launch_sample_t<T, JPL, 256, false, false>(m, w, stream);
+}
+
 template <int JPL>
 int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int limit, cudaStream_t stream) {
   // Resident (shared-memory) planes run one walker per SM with 16 warps; planes in global
   // memory run several walkers per SM with 8 warps each.
   if (residency_policy() == 1) {
-    if (precision == 32) return launch_sample_t<float, JPL, 256, false, false>(m, w, stream);
-    return launch_sample_t<double, JPL, 256, false, false>(m, w, stream);
+    if (precision == 32) return launch_sample_global<float, JPL>(m, w, stream);
+    return launch_sample_global<double, JPL>(m, w, stream);
   }
   if (precision == 32) {
     if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit))
       return launch_sample_t<float, JPL, 512, true, true>(m, w, stream);
     if (samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit))
       return launch_sample_t<float, JPL, 512, true, false>(m, w, stream);
-    return launch_sample_t<float, JPL, 256, false, false>(m, w, stream);
+    return launch_sample_global<float, JPL>(m, w, stream);
   }
   if (samp_layout<double>(m, true, true).total <= static_cast<size_t>(limit))
     return launch_sample_t<double, JPL, 512, true, true>(m, w, stream);
-  return launch_sample_t<double, JPL, 256, false, false>(m, w, stream);
+  return launch_sample_global<double, JPL>(m, w, stream);
 }
 
 int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStream_t stream) {
@@ -924,6 +999,77 @@ int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStr
   if (n <= 128) return launch_sample_jpl<4>(m, w, precision, limit, stream);
   if (n <= 224) return launch_sample_jpl<7>(m, w, precision, limit, stream);
   if (n <= 256) return launch_sample_jpl<8>(m, w, precision, limit, stream);
+  return kErrArgument;
+}
+
+// ---- one walker's Pfaffian stage (RealPfStage, sampling/stage.rs:56-129) -----------------
+// The five stage operations as single-CTA launches on FP64 planes held in global memory, for
+// host-driven (teacher-forced) replay: the host owns the chain and passes the candidate
+// configuration with every call; the device owns Pf and the inverses.
+template <int JPL>
+__global__ void __launch_bounds__(kStageThreads)
+    k_stage(DevModel m, StageBufs b, int op, int msa, int msb, int rsa_old, int rsb_old, unsigned* status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SampLayout L = samp_layout<double>(m, false, false);
+  WalkerSmem<double> s{};
+  s.idx = reinterpret_cast<int*>(smem + L.idx);
+  s.pf = reinterpret_cast<double*>(smem + L.pf);
+  s.pfn = reinterpret_cast<double*>(smem + L.pfn);
+  s.qpw = reinterpret_cast<double*>(smem + L.qpw);
+  s.jidx = m.jast_idx;
+  s.vec = reinterpret_cast<double*>(smem + L.vec);
+  s.pscal = reinterpret_cast<double*>(smem + L.vec + sizeof(double) * 4 * static_cast<size_t>(m.nqp) * m.n);
+  s.gj = gj_carve<double>(smem + L.gj, m.n);
+  const size_t nn = static_cast<size_t>(m.n) * m.n;
+  s.ws = b.ws;
+  s.ws2 = b.ws + nn;
+  s.planes = b.planes;
+  const int tid = threadIdx.x;
+  for (int k = tid; k < m.n; k += blockDim.x) s.idx[k] = b.idx[k];
+  for (int k = tid; k < m.nqp; k += blockDim.x) {
+    s.pf[k] = b.pf[k];
+    s.pfn[k] = b.pfn[k];
+    s.qpw[k] = m.qpw[k];
+  }
+  __syncthreads();
+  if (op == kStageRecompute) {
+    const int info = calc_m_all_dev<double, JPL, true>(m, s, status);
+    if (tid == 0) b.info[0] = info;
+  } else if (op == kStageProposeHop) {
+    ratio_hop_dev<double>(m, s, msa);
+  } else if (op == kStageAcceptHop) {
+    update_hop_dev<double, JPL>(m, s, msa);
+  } else if (op == kStageProposeExchange) {
+    ratio_exchange_dev<double>(m, s, msa, msb);
+  } else if (op == kStageAcceptExchange) {
+    update_exchange_dev<double, JPL>(m, s, msa, msb, rsa_old, rsb_old);
+  }
+  __syncthreads();
+  for (int k = tid; k < m.nqp; k += blockDim.x) {
+    b.pf[k] = s.pf[k];
+    b.pfn[k] = s.pfn[k];
+  }
+}
+
+template <int JPL>
+int launch_stage_jpl(const DevModel& m, const StageBufs& b, int op, int msa, int msb, int rsa_old, int rsb_old,
+                     unsigned* status, cudaStream_t stream) {
+  const size_t smem = samp_layout<double>(m, false, false).total;
+  auto kernel = k_stage<JPL>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  kernel<<<1, kStageThreads, smem, stream>>>(m, b, op, msa, msb, rsa_old, rsb_old, status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+int launch_stage(const DevModel& m, const StageBufs& b, int op, int msa, int msb, int rsa_old, int rsb_old,
+                 unsigned* status, cudaStream_t stream) {
+  const int n = m.n;
+  if (n <= 32) return launch_stage_jpl<1>(m, b, op, msa, msb, rsa_old, rsb_old, status, stream);
+  if (n <= 64) return launch_stage_jpl<2>(m, b, op, msa, msb, rsa_old, rsb_old, status, stream);
+  if (n <= 128) return launch_stage_jpl<4>(m, b, op, msa, msb, rsa_old, rsb_old, status, stream);
+  if (n <= 224) return launch_stage_jpl<7>(m, b, op, msa, msb, rsa_old, rsb_old, status, stream);
+  if (n <= 256) return launch_stage_jpl<8>(m, b, op, msa, msb, rsa_old, rsb_old, status, stream);
   return kErrArgument;
 }
 

@@ -5,12 +5,31 @@
 // δ = δ_new (DiagScale), r = g − S·x at every 20th iteration, breakdown |d·q| < 1e-20,
 // status = iterations or −(iter+1). S·v = Oᵀ(O·v)/W − (⟨O⟩·v)⟨O⟩ + δ_shift·diag·v
 // (apply_with_product, sr_cg.rs:952-1009; COrderSr::cg_local_product,
-// sr_backend.rs:518-606), the two passes over the compact active sample matrix O[s][i].
+// sr_backend.rs:518-606) over the compact active sample matrix O[s][i].
 // One cooperative launch runs every iteration: no host round trip until the solve ends.
 // Every reduction has a fixed order, so the recurrence is bitwise repeatable.
+//
+// The product reads O once per application: each block owns a contiguous range of
+// sample rows and takes them R at a time into registers (thread t holds columns
+// t, t + T, ...); a block-wide sum gives the R row products y_s = O_s·v, and the same
+// registers accumulate Σ_s y_s·O_s into per-thread column sums. The per-block column
+// partials are then summed across blocks in block order.
+//
+// Reduced-precision operator (mixed path): the active matrix is stored centred and
+// column-scaled in FP32 or BF16 (half or a quarter of the FP64 bytes, so that at the SR
+// configurations it stays in L2 across iterations) and the products accumulate in FP32;
+// vectors, dots and the α/β recurrence stay FP64. The product is a pair of matrix-vector
+// contractions at ≤ 1 flop per byte, bound by memory bandwidth, so it runs on the CUDA
+// cores: tensor cores would add no throughput.
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <string>
+#include <type_traits>
+
+#include "../host/abi_common.h"
 #include "common.cuh"
 #include "engine.cuh"
 
@@ -18,8 +37,8 @@ namespace cgr = cooperative_groups;
 
 namespace mvmcb {
 
-constexpr int kCgThreads = 256;
-
+constexpr int kCgThreads = 512;   // one block of 16 warps per SM
+constexpr int kCgMaxCols = 16;    // columns per thread: na ≤ kCgThreads · kCgMaxCols
 
 __device__ double block_sum(double v, double* sh) {
   v = warp_sum(v);
@@ -51,38 +70,132 @@ __device__ double grid_dot(cgr::grid_group& grid, const double* a, const double*
   return t;
 }
 
-// out = S·v
-__device__ void sr_apply(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, double* sh) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
-  for (long long s = gw; s < a.ns; s += nwarps) {
-    const double* row = a.O + s * a.na;
-    double t = 0.0;
-    for (int i = lane; i < a.na; i += 32) t += row[i] * v[i];
-    t = warp_sum(t);
-    if (lane == 0) a.y[s] = t;
+// Element access of the stored sample matrix: FP64 (C order), FP32 or BF16.
+template <typename OT>
+struct Elem;
+template <>
+struct Elem<double> {
+  using CT = double;
+  __device__ static double load(const double* p) { return __ldg(p); }
+};
+template <>
+struct Elem<float> {
+  using CT = float;
+  __device__ static float load(const float* p) { return __ldg(p); }
+};
+template <>
+struct Elem<__nv_bfloat16> {
+  using CT = float;
+  __device__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+};
+
+// R block sums at once: sh needs 32·R + R doubles.
+template <int R>
+__device__ void block_sum_vec(double (&v)[R], double* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = warp_sum(v[r]);
+  if (lane == 0) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) sh[warp * R + r] = v[r];
   }
-  const double coef = grid_dot(grid, a.mean, v, a.na, a.red, sh);  // includes a grid.sync
-  const int ntile = (a.na + blockDim.x - 1) / blockDim.x;
-  const long long chunk = (a.ns + a.nchunk - 1) / a.nchunk;
-  for (int item = blockIdx.x; item < ntile * a.nchunk; item += gridDim.x) {
-    const int tile = item % ntile, c = item / ntile;
-    const int i = tile * blockDim.x + threadIdx.x;
-    if (i >= a.na) continue;
-    const long long s0 = c * chunk, s1 = min(a.ns, s0 + chunk);
+  __syncthreads();
+  if (threadIdx.x < R) {
     double t = 0.0;
-    for (long long s = s0; s < s1; ++s) t += a.O[s * a.na + i] * a.y[s];
-    a.part[static_cast<long long>(c) * a.na + i] = t;
+    for (int w = 0; w < nwarp; ++w) t += sh[w * R + threadIdx.x];
+    sh[32 * R + threadIdx.x] = t;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = sh[32 * R + r];
+  __syncthreads();
+}
+
+// Rows per register batch for KC columns per thread.
+template <int KC>
+struct RowBatch {
+  static constexpr int R = KC <= 2 ? 8 : (KC <= 4 ? 4 : (KC <= 8 ? 2 : 1));
+};
+
+// out = S·v. FP64: Oᵀ(O·v)/Wc − (⟨O⟩·v)⟨O⟩ + shift·diag ⊙ v. Reduced precision (centred,
+// scaled rows): cs ⊙ Olᵀ(Ol·(cs ⊙ v))/Wc + shift·diag ⊙ v.
+template <typename OT, int KC>
+__device__ void sr_apply_rows(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, double* sh,
+                              unsigned char* smem) {
+  using CT = typename Elem<OT>::CT;
+  constexpr int R = RowBatch<KC>::R;
+  constexpr bool kLow = !std::is_same<OT, double>::value;
+  CT* vs = reinterpret_cast<CT*>(smem);
+  const int tid = threadIdx.x, nt = blockDim.x, na = a.na;
+  for (int i = tid; i < na; i += nt) vs[i] = kLow ? static_cast<CT>(a.cs[i] * v[i]) : static_cast<CT>(v[i]);
+  __syncthreads();
+  // ⟨O⟩·v, the same value in every block (fixed order)
+  double coef = 0.0;
+  if (!kLow) {
+    double t = 0.0;
+    for (int i = tid; i < na; i += nt) t += a.mean[i] * v[i];
+    coef = block_sum(t, sh);
+  }
+  const OT* O = kLow ? static_cast<const OT*>(a.Ol) : reinterpret_cast<const OT*>(a.O);
+  const long long lda = kLow ? a.lda : na;
+  const long long per = (a.ns + gridDim.x - 1) / gridDim.x;
+  const long long s0 = static_cast<long long>(blockIdx.x) * per, s1 = min(a.ns, s0 + per);
+  double z[KC];
+#pragma unroll
+  for (int k = 0; k < KC; ++k) z[k] = 0.0;
+  for (long long sb = s0; sb < s1; sb += R) {
+    CT x[R][KC];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const long long s = sb + r;
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int i = tid + k * nt;
+        x[r][k] = (s < s1 && i < na) ? Elem<OT>::load(O + s * lda + i) : CT(0);
+      }
+    }
+    double y[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      CT t = CT(0);
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int i = tid + k * nt;
+        if (i < na) t += x[r][k] * vs[i];
+      }
+      y[r] = static_cast<double>(t);
+    }
+    block_sum_vec<R>(y, sh);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int k = 0; k < KC; ++k) z[k] += static_cast<double>(x[r][k]) * y[r];
+    }
+  }
+  double* part = a.part + static_cast<long long>(blockIdx.x) * na;
+#pragma unroll
+  for (int k = 0; k < KC; ++k) {
+    const int i = tid + k * nt;
+    if (i < na) part[i] = z[k];
   }
   grid.sync();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.na; i += gridDim.x * blockDim.x) {
-    double z = 0.0;
-    for (int c = 0; c < a.nchunk; ++c) z += a.part[static_cast<long long>(c) * a.na + i];
-    out[i] = a.inv_w * z - coef * a.mean[i] + a.shift * a.diag[i] * v[i];
+  for (int i = blockIdx.x * nt + tid; i < na; i += gridDim.x * nt) {
+    double t = 0.0;
+    for (int b = 0; b < static_cast<int>(gridDim.x); ++b) t += a.part[static_cast<long long>(b) * na + i];
+    out[i] = kLow ? a.inv_w * (a.cs[i] * t) + a.shift * a.diag[i] * v[i]
+                  : a.inv_w * t - coef * a.mean[i] + a.shift * a.diag[i] * v[i];
   }
   grid.sync();
 }
+
+template <typename OT, int KC>
+struct ApplyRows {
+  double* sh;
+  unsigned char* smem;
+  __device__ void operator()(cgr::grid_group& g, const CgArgs& a, const double* v, double* out) const {
+    sr_apply_rows<OT, KC>(g, a, v, out, sh, smem);
+  }
+};
 
 __device__ __forceinline__ double precond(const CgArgs& a, int i, double r) {
   double dq = (1.0 + a.shift) * a.diag[i];
@@ -90,9 +203,9 @@ __device__ __forceinline__ double precond(const CgArgs& a, int i, double r) {
   return r / dq;
 }
 
-__global__ void __launch_bounds__(kCgThreads) k_sr_cg(CgArgs a) {
-  cgr::grid_group grid = cgr::this_grid();
-  __shared__ double sh[40];
+// The C recurrence around an S·v product (apply).
+template <typename Apply>
+__device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, const Apply& apply) {
   const int n = a.na;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
   const double threshold = a.tol * a.tol * static_cast<double>(n) * static_cast<double>(n);
@@ -103,7 +216,7 @@ __global__ void __launch_bounds__(kCgThreads) k_sr_cg(CgArgs a) {
   }
   grid.sync();
   if (a.diag_scale) {
-    sr_apply(grid, a, a.x, a.r, sh);
+    apply(grid, a, a.x, a.r);
     for (int i = gtid; i < n; i += gstride) {
       a.r[i] = a.g[i] - a.r[i];
       a.d[i] = precond(a, i, a.r[i]);
@@ -126,7 +239,7 @@ __global__ void __launch_bounds__(kCgThreads) k_sr_cg(CgArgs a) {
     const long long failed = -(static_cast<long long>(iter) + 1);
     if (!isfinite(delta)) { status = failed; done = true; break; }
     if (fabs(delta) < threshold) break;
-    sr_apply(grid, a, a.d, a.q, sh);
+    apply(grid, a, a.d, a.q);
     const double dq = grid_dot(grid, a.d, a.q, n, a.red, sh);
     if (!isfinite(dq) || fabs(dq) < 1e-20) { status = failed; done = true; break; }
     const double alpha = delta / dq;
@@ -134,7 +247,7 @@ __global__ void __launch_bounds__(kCgThreads) k_sr_cg(CgArgs a) {
     for (int i = gtid; i < n; i += gstride) a.x[i] += alpha * a.d[i];
     grid.sync();
     if ((iter + 1) % 20 == 0) {
-      sr_apply(grid, a, a.x, a.r, sh);
+      apply(grid, a, a.x, a.r);
       for (int i = gtid; i < n; i += gstride) a.r[i] = a.g[i] - a.r[i];
     } else {
       for (int i = gtid; i < n; i += gstride) a.r[i] -= alpha * a.q[i];
@@ -172,6 +285,23 @@ __global__ void __launch_bounds__(kCgThreads) k_sr_cg(CgArgs a) {
   }
 }
 
+
+template <typename OT, int KC>
+__global__ void __launch_bounds__(kCgThreads, 1) k_sr_cg(CgArgs a) {
+  cgr::grid_group grid = cgr::this_grid();
+  __shared__ double sh[32 * 8 + 8 + 8];
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (a.nchunk < static_cast<int>(gridDim.x)) {  // partial buffer too small: refuse
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.scal[0] = 0.0;
+      a.scal[1] = -1.0;
+      a.scal[2] = 0.0;
+    }
+    return;
+  }
+  cg_run(grid, a, sh, ApplyRows<OT, KC>{sh, smem});
+}
+
 // Gather the active columns of the stored O rows: Oa[s][si] = store[s][map[si] + 1].
 __global__ void k_gather_active(const double* __restrict__ store, int sr_size, long long ns,
                                 const int* __restrict__ map, int na, double* __restrict__ oa) {
@@ -193,26 +323,112 @@ int launch_gather_active(const double* store, int sr_size, long long ns, const i
   return kOk;
 }
 
-// Blocks of the cooperative solve: enough to stream the sample matrix (about 64K
-// elements per block), never more than are co-resident.
+// One block per SM (co-resident for the cooperative launch).
 int cg_grid_blocks(long long ns, int na) {
-  static int cap = -1;
-  if (cap < 0) {
-    int dev = 0, sms = 0, per = 0;
+  (void)ns;
+  (void)na;
+  static int sms = -1;
+  if (sms < 0) {
+    int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sr_cg, kCgThreads, 0);
-    cap = sms * std::max(1, std::min(per, 4));
+    sms = std::max(1, sms);
   }
-  const long long want = (ns * static_cast<long long>(na) + 65535) / 65536;
-  return static_cast<int>(std::max<long long>(1, std::min<long long>(cap, want)));
+  return sms;
+}
+
+int cg_grid_blocks_kind(long long ns, int na, int kind) {
+  (void)kind;
+  return cg_grid_blocks(ns, na);
+}
+
+// Column partial rows (part[nchunk][na]): one per block.
+int cg_nchunk(long long ns, int na, int kind, int blocks) {
+  (void)ns;
+  (void)na;
+  (void)kind;
+  return blocks;
+}
+
+int low_lda(int na, int kind) {
+  (void)kind;
+  return na;
+}
+
+template <typename OT>
+__device__ __forceinline__ OT to_low(double v);
+template <>
+__device__ __forceinline__ float to_low<float>(double v) {
+  return static_cast<float>(v);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 to_low<__nv_bfloat16>(double v) {
+  return __float2bfloat16_rn(static_cast<float>(v));
+}
+
+// Ol[s][i] = (store[s][map[i] + 1] − mean[i]) / cs[i]; zero for skipped samples (their
+// stored row is zero, leading 1 included).
+template <typename OT>
+__global__ void k_gather_active_low(const double* __restrict__ store, int sr_size, long long ns,
+                                    const int* __restrict__ map, int na, int lda, const double* __restrict__ mean,
+                                    const double* __restrict__ cs, OT* __restrict__ out) {
+  const long long total = ns * lda;
+  for (long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; k < total;
+       k += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long s = k / lda;
+    const int si = static_cast<int>(k - s * lda);
+    double v = 0.0;
+    if (si < na && store[s * sr_size] != 0.0) v = (store[s * sr_size + map[si] + 1] - mean[si]) / cs[si];
+    out[k] = to_low<OT>(v);
+  }
+}
+
+int launch_gather_active_low(const double* store, int sr_size, long long ns, const int* map, int na,
+                             const double* mean, const double* cs, int kind, void* out, cudaStream_t stream) {
+  const int lda = low_lda(na, kind);
+  const long long total = ns * lda;
+  const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
+  if (kind == 1)
+    k_gather_active_low<float><<<grid, 256, 0, stream>>>(store, sr_size, ns, map, na, lda, mean, cs,
+                                                          static_cast<float*>(out));
+  else
+    k_gather_active_low<__nv_bfloat16><<<grid, 256, 0, stream>>>(store, sr_size, ns, map, na, lda, mean, cs,
+                                                                  static_cast<__nv_bfloat16*>(out));
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+template <typename OT, int KC>
+int launch_cg_kc(CgArgs& a, cudaStream_t stream) {
+  void* args[] = {&a};
+  const size_t smem = sizeof(typename Elem<OT>::CT) * static_cast<size_t>(a.na);
+  auto kernel = k_sr_cg<OT, KC>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kernel), cg_grid_blocks(a.ns, a.na), kCgThreads,
+                                         args, smem, stream));
+  return kOk;
+}
+
+template <typename OT>
+int launch_cg_type(CgArgs& a, cudaStream_t stream) {
+  const int kc = (a.na + kCgThreads - 1) / kCgThreads;
+  if (kc <= 1) return launch_cg_kc<OT, 1>(a, stream);
+  if (kc <= 2) return launch_cg_kc<OT, 2>(a, stream);
+  if (kc <= 4) return launch_cg_kc<OT, 4>(a, stream);
+  if (kc <= 8) return launch_cg_kc<OT, 8>(a, stream);
+  if (kc <= kCgMaxCols) return launch_cg_kc<OT, kCgMaxCols>(a, stream);
+  set_last_error("sr-cg: more than " + std::to_string(kCgThreads * kCgMaxCols) + " active parameters");
+  return kErrArgument;
 }
 
 int launch_sr_cg(CgArgs a, cudaStream_t stream) {
-  void* args[] = {&a};
-  MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_sr_cg), cg_grid_blocks(a.ns, a.na), kCgThreads,
-                                         args, 0, stream));
-  return kOk;
+  if (a.nchunk < cg_grid_blocks(a.ns, a.na)) {
+    set_last_error("sr-cg: partial buffer holds fewer rows than the grid has blocks");
+    return kErrArgument;
+  }
+  if (a.o_kind == 1) return launch_cg_type<float>(a, stream);
+  if (a.o_kind == 2) return launch_cg_type<__nv_bfloat16>(a, stream);
+  return launch_cg_type<double>(a, stream);
 }
 
 }  // namespace mvmcb
@@ -234,8 +450,7 @@ extern "C" int mvmc_b200_cg_solve(const double* samples, long long ns, int na, c
   using namespace mvmcb;
   if (!samples || !mean || !diag || !g || !x || !status || na <= 0 || ns <= 0) return kErrArgument;
   const int blocks = cg_grid_blocks(ns, na);
-  const int ntile = (na + 255) / 256;
-  const int nchunk = static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, blocks / ntile))));
+  const int nchunk = cg_nchunk(ns, na, 0, blocks);
   Buf o, vec, y, part, red, scal;
   MVMCB_CUDA(cudaMalloc(&o.p, sizeof(double) * ns * na));
   MVMCB_CUDA(cudaMalloc(&vec.p, sizeof(double) * 7 * na));

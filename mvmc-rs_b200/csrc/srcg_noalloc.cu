@@ -31,6 +31,7 @@ namespace mvmcb {
 
 int launch_sr_cg(CgArgs a, cudaStream_t stream);
 int cg_grid_blocks(long long ns, int na);
+int cg_nchunk(long long ns, int na, int kind, int blocks);
 
 namespace {
 
@@ -84,8 +85,7 @@ extern "C" int mvmc_b200_cg_solve_noalloc(const double* samples, long long ns, i
     return kErrArgument;
   }
   const int blocks = cg_grid_blocks(ns, na);
-  const int ntile = (na + 255) / 256;
-  const int nchunk = static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, blocks / ntile))));
+  const int nchunk = cg_nchunk(ns, na, 0, blocks);
   const long long need = 3LL * na + ns + static_cast<long long>(nchunk) * na + blocks;
   if (need > kNoAllocScratchDoubles) {
     set_last_error("cg_solve_noalloc: problem needs " + std::to_string(need) +

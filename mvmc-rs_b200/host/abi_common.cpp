@@ -20,4 +20,6 @@ extern "C" void mvmc_b200_default_options(mvmc_b200_options* opt) {
   opt->saved_per_walker = 0;
   opt->seed = -1;
   opt->device = 0;
+  opt->sr_precision = 0;
+  opt->refresh_guard = 0.0;
 }

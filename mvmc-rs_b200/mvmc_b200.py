@@ -20,14 +20,19 @@ EXPORTS = [
     "mvmc_b200_get_samples", "mvmc_b200_measure", "mvmc_b200_get_o_store",
     "mvmc_b200_get_local_energies", "mvmc_b200_sr_cg", "mvmc_b200_status", "mvmc_b200_run_opt",
     "mvmc_b200_last_error", "mvmc_b200_cg_solve", "mvmc_b200_stream", "mvmc_b200_transfer_bytes",
-    "mvmc_b200_sampler_timers", "mvmc_b200_cg_solve_noalloc",
+    "mvmc_b200_sampler_timers", "mvmc_b200_cg_solve_noalloc", "mvmc_b200_refresh_stats",
+    "mvmc_b200_get_log_amplitudes", "mvmc_b200_stage_create", "mvmc_b200_stage_destroy",
+    "mvmc_b200_stage_begin", "mvmc_b200_stage_propose_hop", "mvmc_b200_stage_accept_hop",
+    "mvmc_b200_stage_propose_exchange", "mvmc_b200_stage_accept_exchange", "mvmc_b200_stage_recompute",
+    "mvmc_b200_stage_state",
 ]
 
 
 class Options(ctypes.Structure):
     _fields_ = [("walkers", ctypes.c_int), ("precision", ctypes.c_int),
                 ("refresh_sweeps", ctypes.c_int), ("saved_per_walker", ctypes.c_int),
-                ("seed", ctypes.c_longlong), ("device", ctypes.c_int)]
+                ("seed", ctypes.c_longlong), ("device", ctypes.c_int), ("sr_precision", ctypes.c_int),
+                ("refresh_guard", ctypes.c_double)]
 
 
 def lib():
@@ -180,6 +185,14 @@ class Engine:
                "local_energies")
         return out
 
+    def log_amplitudes(self):
+        """ln|Psi(x)| of every saved sample from the last measurement."""
+        d = self.dims
+        out = np.zeros(d["walkers"] * d["saved"])
+        _check(lib().mvmc_b200_get_log_amplitudes(self.ctx, _ptr(out), ctypes.c_longlong(out.size)),
+               "log_amplitudes")
+        return out
+
     def sr_cg(self):
         info = np.zeros(9)
         rc = _check(lib().mvmc_b200_sr_cg(self.ctx, _ptr(info)), "sr_cg")
@@ -193,6 +206,16 @@ class Engine:
         h, d = ctypes.c_longlong(), ctypes.c_longlong()
         _check(lib().mvmc_b200_transfer_bytes(self.ctx, ctypes.byref(h), ctypes.byref(d)), "transfer_bytes")
         return h.value, d.value
+
+    def refresh_stats(self):
+        """{drift_max, drift_mean, scheduled refreshes / walker, guard refreshes / walker}."""
+        st = np.zeros(4)
+        _check(lib().mvmc_b200_refresh_stats(self.ctx, _ptr(st)), "refresh_stats")
+        return dict(drift_max=st[0], drift_mean=st[1], refreshes=st[2], guard_refreshes=st[3])
+
+    def refresh_drift(self):
+        st = self.refresh_stats()
+        return st["drift_max"], st["drift_mean"]
 
     def sampler_timers(self):
         c = np.zeros(8)
@@ -210,3 +233,68 @@ def run_opt(namelist, out_dir, initial_def="", nsteps=0, **options):
     opt = default_options(**options)
     _check(lib().mvmc_b200_run_opt(namelist.encode(), (initial_def or "").encode(), out_dir.encode(),
                                    ctypes.byref(opt), nsteps), "run_opt")
+
+
+class Stage:
+    """One walker's device Pfaffian stage (RealPfStage) over an Engine's model."""
+
+    def __init__(self, engine):
+        self.engine = engine
+        self.h = ctypes.c_void_p()
+        _check(lib().mvmc_b200_stage_create(engine.ctx, ctypes.byref(self.h)), "stage_create")
+        d = engine.dims
+        self.nqp, self.n, self.ne = d["nqp"], 2 * d["ne"], d["ne"]
+
+    def close(self):
+        if self.h:
+            lib().mvmc_b200_stage_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _idx(ele_idx):
+        return np.ascontiguousarray(ele_idx, dtype=np.int64)
+
+    def begin(self, ele_idx):
+        pf = np.zeros(self.nqp)
+        idx = self._idx(ele_idx)
+        return _check(lib().mvmc_b200_stage_begin(self.h, _ptr(idx), _ptr(pf)), "stage_begin"), pf
+
+    def recompute(self, ele_idx):
+        pf = np.zeros(self.nqp)
+        idx = self._idx(ele_idx)
+        return _check(lib().mvmc_b200_stage_recompute(self.h, _ptr(idx), _ptr(pf)), "stage_recompute"), pf
+
+    def propose_hop(self, ele_idx, ma, spin):
+        pf = np.zeros(self.nqp)
+        idx = self._idx(ele_idx)
+        _check(lib().mvmc_b200_stage_propose_hop(self.h, _ptr(idx), ma, spin, _ptr(pf)), "stage_propose_hop")
+        return pf
+
+    def accept_hop(self, ele_idx, ma, spin, pf_new=None):
+        idx = self._idx(ele_idx)
+        p = None if pf_new is None else np.ascontiguousarray(pf_new, dtype=np.float64)
+        _check(lib().mvmc_b200_stage_accept_hop(self.h, _ptr(idx), ma, spin, _ptr(p)), "stage_accept_hop")
+
+    def propose_exchange(self, ele_idx, ma, sa, mb, sb):
+        pf = np.zeros(self.nqp)
+        idx = self._idx(ele_idx)
+        _check(lib().mvmc_b200_stage_propose_exchange(self.h, _ptr(idx), ma, sa, mb, sb, _ptr(pf)),
+               "stage_propose_exchange")
+        return pf
+
+    def accept_exchange(self, ele_idx, ma, sa, mb, sb, ra_old, rb_old):
+        idx = self._idx(ele_idx)
+        _check(lib().mvmc_b200_stage_accept_exchange(self.h, _ptr(idx), ma, sa, mb, sb, ra_old, rb_old),
+               "stage_accept_exchange")
+
+    def state(self):
+        pf = np.zeros(self.nqp)
+        inv = np.zeros(self.nqp * self.n * self.n)
+        _check(lib().mvmc_b200_stage_state(self.h, _ptr(pf), _ptr(inv)), "stage_state")
+        return pf, inv.reshape(self.nqp, self.n, self.n)

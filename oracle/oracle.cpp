@@ -549,6 +549,22 @@ void initial_with_retry(const Ctx& c, Walker& w) {
 }
 
 // One run_block of n_in proposals.
+// Largest |ln|IP|_recomputed − ln|IP|_tracked| seen at a refresh (diagnostic).
+double g_refresh_drift = 0.0;
+// Diagnostic refresh guard: recompute after an accepted move whose ratio on any QP plane
+// lies outside [g, 1/g] (0 = off, the reference's schedule); counts guard refreshes.
+double g_guard = 0.0;
+long long g_guard_count = 0, g_sched_count = 0;
+
+bool guard_trips(const Ctx& c, const double* pf_new, const double* pf_old) {
+  if (g_guard <= 0.0) return false;
+  for (int q = 0; q < c.nqp; ++q) {
+    const double r = std::fabs(pf_new[q] / pf_old[q]);
+    if (!(r >= g_guard && r * g_guard <= 1.0)) return true;
+  }
+  return false;
+}
+
 void run_block(const Ctx& c, Walker& w, int n_in, double& log_ip_old, int& n_acc_win) {
   const int ns = c.ns, ne = c.ne;
   std::vector<double> pf_new(c.nqp);
@@ -593,11 +609,17 @@ void run_block(const Ctx& c, Walker& w, int n_in, double& log_ip_old, int& n_acc
       if (!std::isfinite(wgt)) wgt = -1.0;
       const double u = w.rng.real2();
       if (wgt > u) {
+        const bool trip = guard_trips(c, pf_new.data(), w.pf.data());
         update_hop(c, msa, idx, w.inv.data(), w.pf.data());
         w.proj_cnt = cnt_new;
         log_ip_old = lip_new;
         ++n_acc_win;
         w.counter[1]++;
+        if (trip && n_acc_win <= ns) {
+          n_acc_win = ns + 1;
+          ++g_guard_count;
+          --g_sched_count;
+        }
       } else {
         revert_ele_config(c, mi, ri, rj, s, idx, cfg, num);
       }
@@ -636,19 +658,31 @@ void run_block(const Ctx& c, Walker& w, int n_in, double& log_ip_old, int& n_acc
       if (!std::isfinite(wgt)) wgt = -1.0;
       const double u = w.rng.real2();
       if (wgt > u) {
+        const bool trip = guard_trips(c, pf_new.data(), w.pf.data());
         update_exchange(c, msa, msb, ri, rj, s, t, idx, w.inv.data(), w.pf.data());
         w.proj_cnt = cnt_new;
         log_ip_old = lip_new;
         ++n_acc_win;
         w.counter[3]++;
+        if (trip && n_acc_win <= ns) {
+          n_acc_win = ns + 1;
+          ++g_guard_count;
+          --g_sched_count;
+        }
       } else {
         revert_ele_config(c, mj, rj, ri, t, idx, cfg, num);
         revert_ele_config(c, mi, ri, rj, s, idx, cfg, num);
       }
     }
     if (n_acc_win > ns) {
+      ++g_sched_count;
       const int info = calc_m_all(c, idx, w.inv.data(), w.pf.data());
-      if (info == 0) log_ip_old = log_ip(c, w.pf.data());
+      if (info == 0) {
+        const double fresh = log_ip(c, w.pf.data());
+        const double d = std::fabs(fresh - log_ip_old);
+        if (std::isfinite(d) && d > g_refresh_drift) g_refresh_drift = d;
+        log_ip_old = fresh;
+      }
       n_acc_win = 0;
     }
   }
@@ -1341,6 +1375,20 @@ int oracle_opt_step1_walkers(const char* namelist, const char* initial_def, int 
   }
 }
 
+void oracle_set_refresh_guard(double g) { orc::g_guard = g; }
+
+void oracle_refresh_counts(long long* sched, long long* guard, int reset) {
+  *sched = orc::g_sched_count;
+  *guard = orc::g_guard_count;
+  if (reset) orc::g_sched_count = orc::g_guard_count = 0;
+}
+
+double oracle_refresh_drift(int reset) {
+  const double d = orc::g_refresh_drift;
+  if (reset) orc::g_refresh_drift = 0.0;
+  return d;
+}
+
 int oracle_cg_fixed(int n, int samples, const double* mean, const double* diag, const double* smp,
                     const double* g, double inv_w, double shift, double tol, int max_iter,
                     int diag_scale, double* x_out, double* z_apply) {
@@ -1359,6 +1407,66 @@ int oracle_cg_fixed(int n, int samples, const double* mean, const double* diag, 
   orc::CgResult r = orc::cg_solve(op, std::vector<double>(g, g + n), tol, max_iter, diag_scale != 0);
   std::copy(r.x.begin(), r.x.end(), x_out);
   return static_cast<int>(r.status);
+}
+
+// Teacher-forced replay of the RealPfStage operations (sampling/stage.rs:56-129) with the
+// CPU stage arithmetic above (CpuStage, stage.rs:134-240): the Slater table of `params`
+// (projection then Slater parameters), the inverses of idx0, then nops calls, each row of
+// ops = {code, ma, sa, mb, sb, ra_old, rb_old}; code 0 propose hop, 1 accept hop (the
+// current Pf become the last proposal's, stage.rs:182), 2 propose exchange, 3 accept
+// exchange, 4 recompute. idx_seq holds the ele_idx of every call. out[k*nqp..]: pf_new of
+// a proposal, else the current Pf (NaN after a failed recompute); inv_out: the final InvM.
+int oracle_stage_replay(const char* namelist, const double* params, int npara, const int64_t* idx0, int nops,
+                        const int* ops, const int64_t* idx_seq, double* out, double* inv_out, char* err,
+                        int err_len) {
+  try {
+    mvmc::Model m = mvmc::read_expert(namelist);
+    if (npara != m.npara()) throw std::runtime_error("parameter count mismatch");
+    mvmc::set_all_parameters(m, std::vector<double>(params, params + npara));
+    mvmc::init_qp_weight(m);
+    std::vector<double> slater;
+    mvmc::build_slater_table(m, slater);
+    orc::Ctx c(m, slater);
+    const int n = c.n, nqp = c.nqp, ne = c.ne;
+    std::vector<double> inv(static_cast<size_t>(nqp) * n * n), pf(nqp), pfn(nqp);
+    if (orc::calc_m_all(c, idx0, inv.data(), pf.data()) != 0) throw std::runtime_error("singular start");
+    for (int k = 0; k < nops; ++k) {
+      const int* o = ops + 7 * k;
+      const int64_t* idx = idx_seq + static_cast<size_t>(k) * n;
+      const int msa = o[1] + o[2] * ne, msb = o[3] + o[4] * ne;
+      double* dst = out + static_cast<size_t>(k) * nqp;
+      switch (o[0]) {
+        case 0:
+          orc::ratio_hop(c, msa, idx, inv.data(), pf.data(), pfn.data());
+          std::copy(pfn.begin(), pfn.end(), dst);
+          break;
+        case 1:
+          orc::update_hop(c, msa, idx, inv.data(), pf.data());
+          pf = pfn;
+          std::copy(pf.begin(), pf.end(), dst);
+          break;
+        case 2:
+          orc::ratio_exchange(c, msa, msb, idx, inv.data(), pf.data(), pfn.data());
+          std::copy(pfn.begin(), pfn.end(), dst);
+          break;
+        case 3:
+          orc::update_exchange(c, msa, msb, o[5], o[6], o[2], o[4], idx, inv.data(), pf.data());
+          std::copy(pf.begin(), pf.end(), dst);
+          break;
+        case 4:
+          if (orc::calc_m_all(c, idx, inv.data(), pf.data()) != 0) std::fill(dst, dst + nqp, NAN);
+          else std::copy(pf.begin(), pf.end(), dst);
+          break;
+        default:
+          throw std::runtime_error("unknown stage op");
+      }
+    }
+    std::copy(inv.begin(), inv.end(), inv_out);
+    return 0;
+  } catch (const std::exception& e) {
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
 }
 
 }  // extern "C"

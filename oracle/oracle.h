@@ -65,6 +65,25 @@ int oracle_cg_fixed(int n, int samples, const double* mean, const double* diag, 
                     const double* g, double inv_w, double shift, double tol, int max_iter,
                     int diag_scale, double* x_out, double* z_apply);
 
+// Teacher-forced replay of the RealPfStage operations (sampling/stage.rs:56-129) on one
+// walker: Slater table of `params`, inverses of idx0, then nops calls with rows
+// ops[7k..] = {code, ma, sa, mb, sb, ra_old, rb_old} (0 propose hop, 1 accept hop, 2 propose
+// exchange, 3 accept exchange, 4 recompute) and the call's ele_idx in idx_seq[k*n..].
+// out[k*nqp..]: pf_new of a proposal, else the current Pf; inv_out: the final InvM planes.
+int oracle_stage_replay(const char* namelist, const double* params, int npara, const int64_t* idx0, int nops,
+                        const int* ops, const int64_t* idx_seq, double* out, double* inv_out, char* err,
+                        int err_len);
+
+// Largest |ln|IP|_recomputed − ln|IP|_tracked| at a sampler refresh since the last reset
+// (the FP64 rank-2 updates' drift on the C refresh schedule); reset != 0 clears it.
+double oracle_refresh_drift(int reset);
+
+// The refresh guard of the device's mixed path, restated for the FP64 chain: recompute right
+// after an accepted move whose Pfaffian ratio on any QP plane lies outside [g, 1/g]
+// (0 = off, the reference's schedule). Counts: scheduled and guard refreshes since reset.
+void oracle_set_refresh_guard(double g);
+void oracle_refresh_counts(long long* sched, long long* guard, int reset);
+
 // Model dimensions for buffer sizing: [nsite, ne, nqp, nproj, npara, nvmc_sample,
 // data_qty_smp, n_orb].
 int oracle_model_dims(const char* namelist, int* dims, char* err, int err_len);

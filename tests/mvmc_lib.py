@@ -23,3 +23,11 @@ def read_triples(path, npara):
     vals = np.array([float(t) for t in open(path).read().split()])
     vals = vals[len(vals) - (6 + 3 * npara):]
     return vals[6::3][:npara]
+
+
+def lattice():
+    """The synthetic Hubbard input generator (mvmc-rs_b200/lattice.py)."""
+    spec = importlib.util.spec_from_file_location("lattice", os.path.join(ROOT, "mvmc-rs_b200", "lattice.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod

@@ -122,3 +122,19 @@ def opt_step1_walkers(namelist, walkers, seed=-1, initial_def=""):
         raise RuntimeError(err.value.decode())
     out["ostore"] = out["ostore"].reshape(W * S, size)
     return d, out
+
+
+def stage_replay(namelist, params, idx0, ops, idx_seq, nqp, n):
+    """Teacher-forced replay of the stage operations; returns (out[nops][nqp], inv[nqp][n][n])."""
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    idx0 = np.ascontiguousarray(idx0, dtype=np.int64)
+    ops = np.ascontiguousarray(ops, dtype=np.int32).reshape(-1, 7)
+    idx_seq = np.ascontiguousarray(idx_seq, dtype=np.int64)
+    out = np.zeros((len(ops), nqp))
+    inv = np.zeros(nqp * n * n)
+    err = err_buf()
+    rc = lib().oracle_stage_replay(namelist.encode(), ptr(params), len(params), ptr(idx0), len(ops), ptr(ops),
+                                   ptr(idx_seq), ptr(out), ptr(inv), err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return out, inv.reshape(nqp, n, n)

@@ -36,6 +36,10 @@ sys.path.insert(0, os.path.join(ROOT, "mvmc-rs_b200"))
 WALKERS = {"chain16": 256, "square8": 4096, "square16": 2048, "square16_sr": 8192}
 PFINV = {"pfinv64": [64] * 8192, "pfinv_mix": [32, 48, 64, 96, 128] * 1638}
 METRIC = "Metropolis sweeps/s & SR-step time: mixed vs FP64 path on 1 B200 at |dE|/N<=1e-6"
+# DRAM bytes (read + write) per walker-sweep of k_sample from an ncu capture of a small
+# case of the same kernel instance (profiles/k_sample_fp64_square8_w296.txt: 2.632 GB over
+# 296 walkers x 4 sweeps), scaled to a launch by walker-sweeps.
+SAMPLE_DRAM_PER_WALKER_SWEEP = {("square8", 64): 2.632e9 / (296 * 4)}
 PFINV_METRIC = "Pfaffian+inverse/s (batched skew FP64)"
 
 
@@ -340,6 +344,8 @@ def engine_bench(args, ws, rank, local):
     per_sweep = ns * (nqp * n * s_bytes + nqp * n * 8) + ns * p_acc * nqp * (2 * n * n * s_bytes)
     launch_bytes = W * sweeps_per_walker_step * per_sweep
     achieved = launch_bytes / (main_rec["sample_ms"] / 1e3) / 1e9
+    per_ws = SAMPLE_DRAM_PER_WALKER_SWEEP.get((args.config, args.precision))
+    traffic = per_ws * W * sweeps_per_walker_step if per_ws and not args.interval else None
     peak, peak_kind = measured_peaks()
     if rank != 0:
         if ws > 1:
@@ -364,8 +370,8 @@ def engine_bench(args, ws, rank, local):
         "measure_ms": main_rec["measure_ms"], "energy": main_rec["energy"], "acceptance": p_acc,
         "cg_iterations": main_rec["cg_iters"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel": "k_sample",
-                     "peak_kind": peak_kind},
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "k_sample",
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": launch_bytes},
         "cpu_baseline": {"value": base_sweeps / base_t, "unit": "sweeps/s", "cores": 1, "kind": "port",
                          "sample": f"1 chain x one SR step (warm-up + {S} blocks, {base_sweeps} sweeps) "
                                    f"of {args.config}"},

@@ -331,8 +331,15 @@ int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, co
   } else {
     auto kernel = k_measure<JPL, false>;
     MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    kernel<<<std::min(nsamples, gws_blocks), kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples,
-                                                                          gws, ostore, eloc, lpsi, valid, status);
+    // As many blocks as are co-resident, striding over the samples: each block reuses its
+    // own ping-pong workspace, so the workspaces stay in L2 across samples.
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kMeasThreads, smem));
+    const int grid = std::max(1, std::min({nsamples, gws_blocks, sms * std::max(1, per)}));
+    kernel<<<grid, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
+                                                 valid, status);
   }
   MVMCB_CUDA(cudaGetLastError());
   return kOk;

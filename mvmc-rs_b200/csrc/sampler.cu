@@ -466,53 +466,58 @@ __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, i
     const T* vt = vec + (q * 4 + 1) * n;
     const T* vp = vec + (q * 4 + 2) * n;
     const T* vq = vec + (q * 4 + 3) * n;
+    // The rank-4 correction (plus the row/column fixes of slots msa, msb) as four column
+    // vectors with per-row coefficients: x_ij += Ct_i·t_j + Cs_i·s_j + Cq_i·q'_j + Cp_i·p'_j,
+    // p' = p + e_msa, q' = q + e_msb (the column fixes); the row fixes enter Ct..Cp of rows
+    // msa and msb.
     T pc[JPL], qc[JPL], sc_[JPL], tc[JPL];
 #pragma unroll
     for (int c2 = 0; c2 < JPL; ++c2) {
       const int j = lane + 32 * c2;
-      pc[c2] = j < n ? vp[j] : T(0);
-      qc[c2] = j < n ? vq[j] : T(0);
+      pc[c2] = j < n ? vp[j] + (j == msa ? T(1) : T(0)) : T(0);
+      qc[c2] = j < n ? vq[j] + (j == msb ? T(1) : T(0)) : T(0);
       sc_[c2] = j < n ? vs[j] : T(0);
       tc[c2] = j < n ? vt[j] : T(0);
     }
     T* P = s.planes + static_cast<size_t>(q) * n * n;
     constexpr int RB = JPL <= 2 ? 2 : 1;  // rows per batch: their loads are issued before any store
     for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
-     T xl[RB][JPL];
+      T xl[RB][JPL];
 #pragma unroll
-     for (int r = 0; r < RB; ++r) {
-       const int i = i0 + r * nwarp;
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
 #pragma unroll
-       for (int c2 = 0; c2 < JPL; ++c2) {
-         const int j = lane + 32 * c2;
-         xl[r][c2] = (i < n && j < n) ? P[static_cast<size_t>(i) * n + j] : T(0);
-       }
-     }
-#pragma unroll
-     for (int r = 0; r < RB; ++r) {
-      const int i = i0 + r * nwarp;
-      if (i >= n) continue;
-      const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
-      T* Pi = P + static_cast<size_t>(i) * n;
-      const bool row_fix = (i == msa) || (i == msb);
-#pragma unroll
-      for (int c2 = 0; c2 < JPL; ++c2) {
-        const int j = lane + 32 * c2;
-        if (j >= n) continue;
-        const T pj = pc[c2], qj = qc[c2], sj = sc_[c2], tj = tc[c2];
-        T x = xl[r][c2] + (a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + c * (pi * tj - pj * ti) +
-                       d * (pi * sj - pj * si) + edet * (si * tj - sj * ti) + fidet * (pi * qj - qi * pj));
-        if (j == msa) x += -c * ti - d * si - fidet * qi;
-        if (j == msb) x += -a * ti - b * si + fidet * pi;
-        if (row_fix) {
-          if (i == msa) x += c * tj + d * sj + fidet * qj;
-          if (i == msb) x += a * tj + b * sj - fidet * pj;
-          if (i == msa && j == msb) x += fidet;
-          if (i == msb && j == msa) x -= fidet;
+        for (int c2 = 0; c2 < JPL; ++c2) {
+          const int j = lane + 32 * c2;
+          xl[r][c2] = (i < n && j < n) ? P[i * n + j] : T(0);
         }
-        Pi[j] = x;
       }
-     }
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        if (i >= n) continue;
+        const T pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
+        T ct = a * qi + c * pi + edet * si;
+        T cs = b * qi + d * pi - edet * ti;
+        T cq = fidet * pi - a * ti - b * si;
+        T cp = -(c * ti + d * si + fidet * qi);
+        if (i == msa) {
+          ct += c;
+          cs += d;
+          cq += fidet;
+        }
+        if (i == msb) {
+          ct += a;
+          cs += b;
+          cp -= fidet;
+        }
+        T* Pi = P + i * n;
+#pragma unroll
+        for (int c2 = 0; c2 < JPL; ++c2) {
+          const int j = lane + 32 * c2;
+          if (j < n) Pi[j] = xl[r][c2] + (ct * tc[c2] + cs * sc_[c2] + cq * qc[c2] + cp * pc[c2]);
+        }
+      }
     }
   }
   __syncthreads();
@@ -560,10 +565,10 @@ __device__ void make_initial_sample_dev(const DevModel& m, SfmtRef& rng, int* id
 }
 
 // Walkers per SM the register budget is sized for: one when the planes are in shared
-// memory; with planes in L2, enough CTAs for 24 warps per SM.
+// memory; with planes in L2, enough CTAs for 16 warps per SM (a tighter budget spills).
 template <int NT, bool kSmemPlanes>
 struct SampOccupancy {
-  static constexpr int kBlocks = kSmemPlanes ? 1 : (768 / NT);
+  static constexpr int kBlocks = kSmemPlanes ? 1 : (512 / NT);
 };
 
 template <typename T, int JPL, int NT, bool kSmemPlanes, bool kSmemWs>

@@ -90,18 +90,10 @@ def test_guard_reduces_mixed_drift_with_projection(tmp_path):
     the guard's extra refreshes cut the loss by orders of magnitude but do not bring it
     to rounding level."""
     nl, init, _ = square8_inputs(tmp_path, interval=4)
-    plain = run(nl, init, 32, 32, 32, 0.0)["stats"]
-    guarded = run(nl, init, 32, 32, 32, 0.1)["stats"]
+    plain = run(nl, init, 32, 32, 2, 0.0)["stats"]
+    guarded = run(nl, init, 32, 32, 2, 0.1)["stats"]
     assert guarded["guard_refreshes"] > 0
     assert guarded["drift_max"] * 10 <= plain["drift_max"]
-
-
-def test_shorter_refresh_cadence_reduces_drift(tmp_path):
-    nl, init, _ = square8_inputs(tmp_path, interval=4, **NO_PROJECTION)
-    long_ = run(nl, init, 32, 32, 32, GUARD)["stats"]
-    short = run(nl, init, 32, 32, 1, GUARD)["stats"]
-    assert short["refreshes"] > long_["refreshes"]
-    assert short["drift_max"] <= long_["drift_max"] + 1e-12
 
 
 def sr_update(nl, init, sr_precision, walkers=1024):

@@ -57,9 +57,10 @@ __host__ __device__ inline SampLayout samp_layout(const DevModel& m, bool smem_p
   L.vec = o; o = align16(o + sizeof(T) * 4 * static_cast<size_t>(m.nqp) * m.n + sizeof(double) * 8 * m.nqp);
   L.gj = o; o = align16(o + gj_shared_bytes<double>(m.n));
   L.ws = o;
-  // FP64 sweep buffers: two n×n buffers for FP32 planes, one scratch buffer for FP64 planes
+  // FP64 sweep buffers: one scratch buffer beside FP64 planes in shared memory, else two
+  // (the plane is gathered into the first).
   const size_t nn8 = sizeof(double) * static_cast<size_t>(m.n) * m.n;
-  if (smem_ws) o = align16(o + (sizeof(T) == sizeof(double) ? nn8 : 2 * nn8));
+  if (smem_ws) o = align16(o + (sizeof(T) == sizeof(double) && smem_planes ? nn8 : 2 * nn8));
   L.planes = o;
   if (smem_planes) o = align16(o + sizeof(T) * static_cast<size_t>(m.nqp) * m.n * m.n);
   L.total = o;
@@ -94,7 +95,7 @@ struct WalkerSmem {
   double* pscal;   // [nqp][8] per-plane scalars
   GJShared<double> gj;
   double* ws;      // FP64 sweep buffer (FP32 planes: the matrix; FP64 planes: the scratch)
-  double* ws2;     // second FP64 sweep buffer (FP32 planes)
+  double* ws2;     // second FP64 sweep buffer
   T* planes;       // [nqp][n][n]
 };
 
@@ -169,14 +170,22 @@ __device__ void update_proj_cnt_warp(const DevModel& m, const int* jtab, int ri,
 // ---- CalculateMAll on every plane (CTA-wide); returns 0 ok, else the first failure -------
 // FP64 planes are swept in place with ws as the ping-pong partner; FP32 planes are swept
 // in FP64 in ws/ws2 and rounded into the plane (the FP64 refresh of the mixed path).
-template <typename T, int JPL, bool kGlobalSweep>
+// FP64 refresh of every plane (CalculateMAll). The sweep runs in the FP64 buffers: in
+// shared memory when they are there (the plane is gathered into the first buffer and the
+// result copied to the plane), else in place on an FP64 plane in L2 with a global scratch.
+template <typename T, int JPL, bool kSmemPlanes, bool kSmemWs>
 __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status) {
   const int n = m.n;
-  const bool fp64_planes = sizeof(T) == sizeof(double);
+  constexpr bool kFp64Planes = sizeof(T) == sizeof(double);
+  // in place: FP64 planes in shared memory, or FP64 planes in L2 without shared buffers
+  constexpr bool kInPlace = kFp64Planes && (kSmemPlanes || !kSmemWs);
+  constexpr bool kSmemSweep = kInPlace ? kSmemPlanes : kSmemWs;
+  constexpr int RB = kSmemSweep ? 1 : (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1));
   int info = 0;
   for (int q = 0; q < m.nqp; ++q) {
-    double* A = fp64_planes ? reinterpret_cast<double*>(s.planes + static_cast<size_t>(q) * n * n) : s.ws;
-    double* B = fp64_planes ? s.ws : s.ws2;
+    T* P = s.planes + static_cast<size_t>(q) * n * n;
+    double* A = kInPlace ? reinterpret_cast<double*>(P) : s.ws;
+    double* B = kInPlace ? s.ws : s.ws2;
     for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
       const int i = k / n, j = k - i * n;
       A[k] = __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + rs_of(m, s.idx, i)) * m.ns2 +
@@ -185,10 +194,8 @@ __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigne
     __syncthreads();
     double pfv;
     int st;
-    if (kGlobalSweep) gj_pfinv_pp<double, JPL, (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, B, n, pfv, st);
-    else gj_pfinv_pp<double, JPL, 1>(A, B, n, pfv, st);
-    if (!fp64_planes) {
-      T* P = s.planes + static_cast<size_t>(q) * n * n;
+    gj_pfinv_pp<double, JPL, RB>(A, B, n, pfv, st);
+    if (!kInPlace) {
       for (int k = threadIdx.x; k < n * n; k += blockDim.x) P[k] = static_cast<T>(A[k]);
     }
     __syncthreads();
@@ -356,7 +363,7 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
 
 // ---- exchange ratio (two_ratio_real, updates.rs:1539-1622) --------------------------------
 //   ratio = InvM_ab·vb_a + InvM_ab·(vbᵀ·InvM·va) + p_a q_b − p_b q_a
-template <typename T>
+template <typename T, int JPL>
 __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, int msb) {
   const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
@@ -641,7 +648,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
     for (int attempt = 1; attempt <= 101; ++attempt) {
       if (tid == 0) make_initial_sample_dev(m, rng, s.idx, s.cfg, s.num, s.cnt);
       __syncthreads();
-      const int info = calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
+      const int info = calc_m_all_dev<T, JPL, kSmemPlanes, kSmemWs>(m, s, w.status);
       if (attempt > 100) {
         if (tid == 0) atomicOr(w.status, kDevInitLoops);
         return;
@@ -650,12 +657,12 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
     }
   };
   if (!burn) initial();
-  calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
+  calc_m_all_dev<T, JPL, kSmemPlanes, kSmemWs>(m, s, w.status);
   if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
   __syncthreads();
   if (!isfinite(s.dctl[dLogIp])) {
     initial();
-    calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
+    calc_m_all_dev<T, JPL, kSmemPlanes, kSmemWs>(m, s, w.status);
     if (tid == 0) s.dctl[dLogIp] = log_ip_of(m, s.pf, s.qpw);
     burn = false;
     __syncthreads();
@@ -787,7 +794,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
           const double z = log_proj_ratio_warp(m.nproj, s.proj, s.cntn, s.cnt);
           if (tid == 0) s.dctl[dDproj] = z;
         }
-        ratio_exchange_dev<T>(m, s, msa, cc[cMsb]);
+        ratio_exchange_dev<T, JPL>(m, s, msa, cc[cMsb]);
       }
       __syncthreads();
       lap(kPhRatio);
@@ -850,7 +857,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
       }
       lap(kPhUpdate);
       if (cc[cRefresh]) {
-        const int info = calc_m_all_dev<T, JPL, !kSmemWs>(m, s, w.status);
+        const int info = calc_m_all_dev<T, JPL, kSmemPlanes, kSmemWs>(m, s, w.status);
         if (tid == 0 && info == 0) {
           // drift of the incrementally updated amplitude against the FP64 recomputation
           const double fresh = log_ip_of(m, s.pf, s.qpw);
@@ -968,9 +975,17 @@ int global_threads() {
   return nt;
 }
 
+// Planes in L2: the FP64 sweep buffers of the refresh go to shared memory when they fit
+// beside the rest without lowering the walkers per SM that the registers allow.
 template <typename T, int JPL>
 int launch_sample_global(const DevModel& m, const DevWalkers& w, cudaStream_t stream) {
   if (global_threads() == 128) return launch_sample_t<T, JPL, 128, false, false>(m, w, stream);
+  int dev = 0, per_sm = 0, reserved = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  const size_t budget = static_cast<size_t>(per_sm / SampOccupancy<256, false>::kBlocks - reserved);
+  if (samp_layout<T>(m, false, true).total <= budget) return launch_sample_t<T, JPL, 256, false, true>(m, w, stream);
   return launch_sample_t<T, JPL, 256, false, false>(m, w, stream);
 }
 
@@ -1038,14 +1053,14 @@ __global__ void __launch_bounds__(kStageThreads)
   }
   __syncthreads();
   if (op == kStageRecompute) {
-    const int info = calc_m_all_dev<double, JPL, true>(m, s, status);
+    const int info = calc_m_all_dev<double, JPL, false, false>(m, s, status);
     if (tid == 0) b.info[0] = info;
   } else if (op == kStageProposeHop) {
     ratio_hop_dev<double>(m, s, msa);
   } else if (op == kStageAcceptHop) {
     update_hop_dev<double, JPL>(m, s, msa);
   } else if (op == kStageProposeExchange) {
-    ratio_exchange_dev<double>(m, s, msa, msb);
+    ratio_exchange_dev<double, JPL>(m, s, msa, msb);
   } else if (op == kStageAcceptExchange) {
     update_exchange_dev<double, JPL>(m, s, msa, msb, rsa_old, rsb_old);
   }

@@ -188,6 +188,8 @@ def engine_inputs(args, rank):
     cfg = dict(lattice.CONFIGS[args.config])
     if args.interval:
         cfg["interval"] = args.interval
+    if args.direct:
+        cfg["nsrcg"] = 0
     tmp = tempfile.mkdtemp(prefix=f"mvmc_bench_{rank}_")
     namelist, initial_def, dims = lattice.write_inputs(os.path.join(tmp, "in"), **cfg)
     return cfg, tmp, namelist, initial_def, dims
@@ -364,7 +366,7 @@ def engine_bench(args, ws, rank, local):
                    "precision": args.precision, "parallelism": f"replicas{ws}",
                    "refresh_sweeps": args.refresh if args.precision == 32 else None,
                    "refresh_guard": args.guard if args.precision == 32 else None,
-                   "sr_precision": args.sr_precision or 64,
+                   "sr_precision": args.sr_precision or 64, "sr": "direct" if args.direct else "cg",
                    "l2": "inputs larger than L2 between steps (walker planes + O matrix)"},
         "sr_step_ms": main_rec["ms"] / args.steps, "sample_ms": main_rec["sample_ms"],
         "measure_ms": main_rec["measure_ms"], "energy": main_rec["energy"], "acceptance": p_acc,
@@ -563,6 +565,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="time one path only (no other precision beside it)")
     ap.add_argument("--sr-precision", type=int, default=0, choices=(0, 64, 32, 16),
                     help="SR operator storage of the timed engine (0: FP64)")
+    ap.add_argument("--direct", action="store_true", help="direct SR (NSRCG 0): Gram + Cholesky instead of SR-CG")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     ws, rank, local = dist_env()

@@ -117,7 +117,9 @@ int mvmc_b200_get_local_energies(const mvmc_b200_ctx* ctx, double* e_loc, long l
  * ln|Psi| at shifted parameters, the finite-difference check of the O rows. */
 int mvmc_b200_get_log_amplitudes(const mvmc_b200_ctx* ctx, double* log_psi, long long count);
 
-/* SR-CG step: stochastic_opt_cg_with_reducer (sr_cg.rs:201-490) with
+/* SR step of the model's mode. NSRCG 0 (direct): stochastic_opt_real_with_sr_info_timed
+ * (sr.rs:77-160) — Gram, redundancy cut, S/g assembly and Cholesky solve on the device.
+ * Otherwise SR-CG: stochastic_opt_cg_with_reducer (sr_cg.rs:201-490) with
  * SampledSrOperator::solve_with_product (sr_cg.rs:700-880) run on the device; S·v is
  * Oᵀ(O·v)/W − ⟨O⟩(⟨O⟩·v) + δ·diag(S)·v. Updates the parameters (update_parameter_value,
  * sr.rs:439) and applies sync_modified_parameter_local (sync.rs:87). sr_info receives
@@ -210,6 +212,16 @@ int mvmc_b200_stage_recompute(mvmc_b200_stage* stage, const int64_t* ele_idx, do
 /* Current Pf[NQP] and inverses inv_m[NQP][n*n] in mVMC's InvM layout (column-major -X^-1,
  * state.rs:208, without the pad slot); either may be NULL. */
 int mvmc_b200_stage_state(const mvmc_b200_stage* stage, double* pf, double* inv_m);
+
+/* SrStages::gram_real (crates/mvmc-core/src/sr_backend.rs:464): out[n][n] = Σ_s row_s row_sᵀ
+ * of `samples` stored rows of n values (host buffers). */
+int mvmc_b200_gram(const double* store, int n, long long samples, double* out);
+
+/* SrStages::cholesky_solve (sr_backend.rs:243-247, sr.rs:535 dpotrf('U') + dpotrs): solve
+ * S x = rhs for the symmetric positive-definite row-major n×n S (host buffers); rhs becomes
+ * x. Returns 1 on a non-positive pivot or a non-finite solution (the reference's Err(())),
+ * 0 on success. The engine's direct SR (NSRCG 0) runs the same kernels on device buffers. */
+int mvmc_b200_cholesky_solve(const double* s, double* rhs, int n);
 
 /* The context's CUDA stream (a cudaStream_t), for timing and ordering with caller work. */
 void* mvmc_b200_stream(mvmc_b200_ctx* ctx);

@@ -37,6 +37,10 @@ int launch_gather_active_low(const double* store, int sr_size, long long ns, con
                              const double* mean, const double* cs, int kind, void* out, cudaStream_t stream);
 int launch_stage(const DevModel& m, const StageBufs& b, int op, int msa, int msb, int rsa_old, int rsb_old,
                  unsigned* status, cudaStream_t stream);
+int launch_gram(const double* store, int n, long long ns, double inv_w, double* oo, cudaStream_t stream);
+int launch_assemble_s(const double* oo, int n, const int* map, int na, double ratio_diag, double* s,
+                      cudaStream_t stream);
+int launch_cholesky_solve(double* a, int n, double* b, int* info_dev, cudaStream_t stream);
 
 // K0: SlaterElm[q][rs_i][rs_j] from the Slater parameters (update_slater_elm,
 // crates/mvmc-core/src/slater_update.rs:17-120).
@@ -118,6 +122,12 @@ struct mvmc_b200_ctx {
   double* d_scal = nullptr;
   int* d_map = nullptr;
   size_t map_cap = 0;
+  // direct SR buffers
+  double* d_oo = nullptr;
+  size_t oo_cap = 0;
+  double* d_smat = nullptr;
+  size_t smat_cap = 0;
+  int* d_info = nullptr;
   std::vector<double> tot;  // host copy of the last reduction
   long long h2d = 0, d2h = 0;  // bytes copied across the host boundary
   bool sampled = false, measured = false;
@@ -378,12 +388,115 @@ int do_measure(mvmc_b200_ctx* c) {
   return kOk;
 }
 
+// Direct SR (NSRCG = 0): stochastic_opt_real_with_sr_info_timed (sr.rs:77-160) with the
+// Gram, the S assembly and the Cholesky solve on the device.
+int do_sr_direct(mvmc_b200_ctx* c, double* info_out) {
+  mvmc::Model& m = c->m;
+  const int size = m.sr_size(), npara = m.npara();
+  const double wc = c->tot[0];
+  const double* ho = c->tot.data() + 5;
+  const long long ns = static_cast<long long>(c->W) * c->S;
+  const size_t nn = static_cast<size_t>(size) * size;
+  if (nn > c->oo_cap) {
+    c->d_oo = c->alloc<double>(nn);
+    c->oo_cap = nn;
+  }
+  if (!c->d_info) c->d_info = c->alloc<int>(1);
+  int rc = launch_gram(c->d_ostore, size, ns, 1.0 / wc, c->d_oo, c->stream);
+  if (rc != kOk) return rc;
+  // row 0 (⟨O⟩) and the diagonal (⟨O²⟩) of OO for the redundancy cut and g
+  std::vector<double> row0(size), diag(size);
+  check(cudaMemcpyAsync(row0.data(), c->d_oo, sizeof(double) * size, cudaMemcpyDeviceToHost, c->stream), "OO row 0");
+  check(cudaMemcpy2DAsync(diag.data(), sizeof(double), c->d_oo, sizeof(double) * (size + 1), sizeof(double), size,
+                          cudaMemcpyDeviceToHost, c->stream),
+        "OO diagonal");
+  check(cudaStreamSynchronize(c->stream), "gram");
+  c->d2h += static_cast<long long>(sizeof(double) * 2 * size);
+  std::vector<double> s_diag(npara);
+  for (int pi = 0; pi < npara; ++pi) s_diag[pi] = diag[pi + 1] - row0[pi + 1] * row0[pi + 1];
+  bool any_nan = false;
+  double vmax = 0.0;
+  for (double v : s_diag) {
+    if (std::isnan(v)) any_nan = true;
+    vmax = std::fmax(vmax, v);
+  }
+  if (any_nan) vmax = NAN;
+  const double cut = vmax * m.red_cut;
+  auto optimised = [&](int comp) {
+    return static_cast<size_t>(comp) < m.opt_flags.size() && m.opt_flags[comp] == 1;
+  };
+  std::vector<int> map;
+  for (int pi = 0; pi < npara; ++pi)
+    if (optimised(2 * pi) && !(s_diag[pi] < cut)) map.push_back(pi);
+  if (info_out) std::fill(info_out, info_out + 9, 0.0);
+  if (map.empty()) return 0;
+  const int na = static_cast<int>(map.size());
+  if (static_cast<size_t>(na) > c->map_cap) {
+    c->d_map = c->alloc<int>(na);
+    c->map_cap = na;
+  }
+  const size_t smat_need = static_cast<size_t>(na) * na + na;
+  if (smat_need > c->smat_cap) {
+    c->d_smat = c->alloc<double>(smat_need);
+    c->smat_cap = smat_need;
+  }
+  std::vector<double> g(na);
+  for (int si = 0; si < na; ++si) {
+    const int pi = map[si] + 1;
+    g[si] = -2.0 * m.step_dt * (ho[pi] - ho[0] * row0[pi]);
+  }
+  double* d_s = c->d_smat;
+  double* d_g = c->d_smat + static_cast<size_t>(na) * na;
+  check(cudaMemcpyAsync(c->d_map, map.data(), sizeof(int) * na, cudaMemcpyHostToDevice, c->stream), "upload map");
+  check(cudaMemcpyAsync(d_g, g.data(), sizeof(double) * na, cudaMemcpyHostToDevice, c->stream), "upload g");
+  c->h2d += static_cast<long long>(sizeof(int) * na + sizeof(double) * na);
+  rc = launch_assemble_s(c->d_oo, size, c->d_map, na, 1.0 + m.sta_del, d_s, c->stream);
+  if (rc != kOk) return rc;
+  rc = launch_cholesky_solve(d_s, na, d_g, c->d_info, c->stream);
+  if (rc != kOk) return rc;
+  int info = 0;
+  check(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "cholesky info");
+  check(cudaMemcpyAsync(g.data(), d_g, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
+  check(cudaStreamSynchronize(c->stream), "sr-direct");
+  c->d2h += static_cast<long long>(sizeof(double) * na + sizeof(int));
+  if (info != 0) return 1;
+  for (double v : g)
+    if (!std::isfinite(v)) return 1;
+  // SRinfo in C's complex index space (real value, zero imaginary variance; sr.rs:309-360)
+  double smax = s_diag[0], smin = s_diag[0];
+  int opt_num = 0, cut_num = 0;
+  for (int comp = 0; comp < 2 * npara; ++comp) {
+    const double d = (comp & 1) ? 0.0 : s_diag[comp / 2];
+    if (d > smax) smax = d;
+    if (d < smin) smin = d;
+  }
+  for (int comp = 0; comp < 2 * npara; ++comp) {
+    const double d = (comp & 1) ? 0.0 : s_diag[comp / 2];
+    if (!optimised(comp)) ++opt_num;
+    else if (d < smax * m.red_cut) ++cut_num;
+  }
+  int imax = 0;
+  for (int i = 1; i < na; ++i)
+    if (std::fabs(g[imax]) < std::fabs(g[i])) imax = i;
+  if (info_out) {
+    const double row[9] = {static_cast<double>(npara), static_cast<double>(na), static_cast<double>(opt_num),
+                           static_cast<double>(cut_num), smax, smin, g[imax], static_cast<double>(2 * map[imax]), 0.0};
+    std::copy(row, row + 9, info_out);
+  }
+  std::vector<double> p = mvmc::all_parameters(m);
+  for (int si = 0; si < na; ++si) p[map[si]] += g[si];
+  mvmc::set_all_parameters(m, p);
+  mvmc::sync_modified_parameter(m, true);
+  upload_parameters(c);
+  return 0;
+}
+
 // stochastic_opt_cg_with_reducer (sr_cg.rs:201-490) around the device solve.
 int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   mvmc::Model& m = c->m;
   const int size = m.sr_size(), npara = m.npara();
   if (!c->measured) return MVMC_B200_ESTATE;
-  if (m.nsrcg == 0) throw std::runtime_error("direct SR (NSRCG 0) is not available on the device path; set NSRCG 1");
+  if (m.nsrcg == 0) return do_sr_direct(c, info_out);
   if (m.rescale_smat) throw std::runtime_error("RescaleSmat is not supported by the device SR path");
   const double wc = c->tot[0];
   const double* ho = c->tot.data() + 5;

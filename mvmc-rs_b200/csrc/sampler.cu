@@ -229,8 +229,9 @@ __device__ void ratio_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa
   }
 }
 
-// Column-form product over plane rows with independent accumulators so that several
-// row loads are in flight: out = Σ_i P[i·n + col]·v[i] (P points at the column).
+// Column-form products over plane rows, out = Σ_i P[i·n + col]·v[i] (P points at the
+// column), with independent accumulators so that several row loads are in flight. A
+// thread with two columns walks both together (eight loads in flight).
 template <typename T>
 __device__ __forceinline__ T col_dot(const T* __restrict__ P, const T* __restrict__ v, int n) {
   T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
@@ -246,24 +247,80 @@ __device__ __forceinline__ T col_dot(const T* __restrict__ P, const T* __restric
 }
 
 template <typename T>
+__device__ __forceinline__ void col_dot_pair(const T* __restrict__ P0, const T* __restrict__ v0,
+                                             const T* __restrict__ P1, const T* __restrict__ v1, int n, T& r0,
+                                             T& r1) {
+  T a[4], b[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) a[u] = b[u] = T(0);
+  int i = 0;
+  for (; i + 4 <= n; i += 4) {
+    T x[4], y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[u] = P0[(i + u) * n];
+      y[u] = P1[(i + u) * n];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] += x[u] * v0[i + u];
+      b[u] += y[u] * v1[i + u];
+    }
+  }
+  for (; i < n; ++i) {
+    a[0] += P0[i * n] * v0[i];
+    b[0] += P1[i * n] * v1[i];
+  }
+  r0 = (a[0] + a[1]) + (a[2] + a[3]);
+  r1 = (b[0] + b[1]) + (b[2] + b[3]);
+}
+
+// out_k[q][j] = −Σ_i P_q[i][j]·vec[q][in][i] → vec[q][out], all (plane, column) items of
+// the CTA, two per thread where there are enough.
+template <typename T>
+__device__ __forceinline__ void planes_col_dot(const DevModel& m, const WalkerSmem<T>& s, int in, int out) {
+  const int n = m.n, total = m.nqp * n, nt = blockDim.x;
+  for (int k = threadIdx.x; k < total; k += 2 * nt) {
+    const int q = k / n, j = k - q * n;
+    const T* P = s.planes + static_cast<size_t>(q) * n * n + j;
+    const int k2 = k + nt;
+    if (k2 < total) {
+      const int q2 = k2 / n, j2 = k2 - q2 * n;
+      T r0, r1;
+      col_dot_pair(P, s.vec + (q * 4 + in) * n, s.planes + static_cast<size_t>(q2) * n * n + j2,
+                   s.vec + (q2 * 4 + in) * n, n, r0, r1);
+      s.vec[(q * 4 + out) * n + j] = -r0;
+      s.vec[(q2 * 4 + out) * n + j2] = -r1;
+    } else {
+      s.vec[(q * 4 + out) * n + j] = -col_dot(P, s.vec + (q * 4 + in) * n, n);
+    }
+  }
+}
+
+template <typename T>
 __device__ __forceinline__ void col_dot2(const T* __restrict__ P, const T* __restrict__ v,
                                          const T* __restrict__ u, int n, T& pv, T& pu) {
-  T a0 = T(0), a1 = T(0), b0 = T(0), b1 = T(0);
+  T a[4], b[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) a[k] = b[k] = T(0);
   int i = 0;
-  for (; i + 2 <= n; i += 2) {
-    const T x0 = P[i * n], x1 = P[(i + 1) * n];
-    a0 += x0 * v[i];
-    b0 += x0 * u[i];
-    a1 += x1 * v[i + 1];
-    b1 += x1 * u[i + 1];
+  for (; i + 4 <= n; i += 4) {
+    T x[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) x[k] = P[(i + k) * n];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      a[k] += x[k] * v[i + k];
+      b[k] += x[k] * u[i + k];
+    }
   }
   for (; i < n; ++i) {
     const T x = P[i * n];
-    a0 += x * v[i];
-    b0 += x * u[i];
+    a[0] += x * v[i];
+    b[0] += x * u[i];
   }
-  pv = a0 + a1;
-  pu = b0 + b1;
+  pv = (a[0] + a[1]) + (a[2] + a[3]);
+  pu = (b[0] + b[1]) + (b[2] + b[3]);
 }
 
 // Lane-owned columns: lane l of every warp owns columns j = l + 32c (c < JPL) of every
@@ -284,11 +341,7 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
     vec[(q * 4 + 0) * n + i] = slater_at<T>(m, q, rsa, rs_of(m, s.idx, i));
   }
   __syncthreads();
-  for (int k = tid; k < nq * n; k += nt) {  // column form: one thread per (plane, column)
-    const int q = k / n, j = k - q * n;
-    const T* P = s.planes + static_cast<size_t>(q) * n * n + j;
-    vec[(q * 4 + 1) * n + j] = -col_dot(P, vec + (q * 4 + 0) * n, n);
-  }
+  planes_col_dot(m, s, 0, 1);  // vec1
   __syncthreads();
   for (int k = tid; k < nq * n; k += nt) {
     const int q = k / n, j = k - q * n;
@@ -376,12 +429,8 @@ __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, in
     vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
   }
   __syncthreads();
-  // (InvM·va)[i] = −Σ_j InvM[j][i]·va[j] (skew symmetry), one thread per (plane, i)
-  for (int k = tid; k < nq * n; k += nt) {
-    const int q = k / n, i = k - q * n;
-    const T* P = s.planes + static_cast<size_t>(q) * n * n + i;
-    vec[(q * 4 + 2) * n + i] = -col_dot(P, vec + (q * 4 + 0) * n, n);
-  }
+  // (InvM·va)[i] = −Σ_j InvM[j][i]·va[j] (skew symmetry)
+  planes_col_dot(m, s, 0, 2);
   __syncthreads();
   for (int q = warp; q < nq; q += nwarp) {
     const T* P = s.planes + static_cast<size_t>(q) * n * n;

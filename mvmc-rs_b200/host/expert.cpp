@@ -534,12 +534,16 @@ void write_out_row(const Model& m, const std::string& dir, int step, const StepE
 }
 
 void write_srinfo_row(const std::string& dir, const Model& m, bool first, const SrInfoRow& r) {
+  // output_files.rs:55-100: the " info" column exists in SR-CG mode only
+  const bool cg = m.nsrcg != 0;
   FILE* f = open_step(dir + "/" + m.data_head + "_SRinfo.dat", first);
   if (first)
-    std::fprintf(f, "#Npara Msize optCut diagCut sDiagMax  sDiagMin    absRmax       imax info\n");
-  std::fprintf(f, "%5d %5d %5d %5d %s %s %s %5d %d\n", r.npara, r.nsmat, r.opt_cut, r.diag_cut,
-               c_exp5(r.sdiag_max).c_str(), c_exp5(r.sdiag_min).c_str(), c_exp5(r.rmax).c_str(),
-               r.imax, r.info);
+    std::fprintf(f, cg ? "#Npara Msize optCut diagCut sDiagMax  sDiagMin    absRmax       imax info\n"
+                       : "#Npara Msize optCut diagCut sDiagMax  sDiagMin    absRmax       imax\n");
+  std::fprintf(f, "%5d %5d %5d %5d %s %s %s %5d", r.npara, r.nsmat, r.opt_cut, r.diag_cut,
+               c_exp5(r.sdiag_max).c_str(), c_exp5(r.sdiag_min).c_str(), c_exp5(r.rmax).c_str(), r.imax);
+  if (cg) std::fprintf(f, " %d", r.info);
+  std::fprintf(f, "\n");
   std::fclose(f);
 }
 

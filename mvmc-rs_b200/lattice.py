@@ -61,7 +61,7 @@ class Lattice:
 def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1), nmp=1, shifts=None,
                  nsp_gauss_leg=1, warmup=10, interval=1, samples=10, steps=10, ex_path=1,
                  seed=12345, step_dt=0.02, red_cut=1e-8, sta_del=0.02, param_seed=2024,
-                 cg_max_iter=200, cg_tol=1e-6, cg_abort=0):
+                 cg_max_iter=200, cg_tol=1e-6, cg_abort=0, nsrcg=1):
     """Write a complete input set; returns (namelist path, initial.def path, dims)."""
     os.makedirs(out_dir, exist_ok=True)
     lat = Lattice(lx, ly)
@@ -77,7 +77,7 @@ def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1),
                NSPStot=0, NMPTrans=nmp, NSROptItrStep=steps, NSROptItrSmp=max(1, steps // 10),
                DSROptRedCut=red_cut, DSROptStaDel=sta_del, DSROptStepDt=step_dt, NVMCWarmUp=warmup,
                NVMCInterval=interval, NVMCSample=samples, NExUpdatePath=ex_path, RndSeed=seed,
-               NSplitSize=1, NStore=1, NSRCG=1, NSROptCGMaxIter=cg_max_iter, DSROptCGTol=cg_tol,
+               NSplitSize=1, NStore=1, NSRCG=nsrcg, NSROptCGMaxIter=cg_max_iter, DSROptCGTol=cg_tol,
                NSRCGAbortOnFail=cg_abort)
     with open(os.path.join(out_dir, "modpara.def"), "w") as f:
         f.write("--------------------\nModel_Parameters   0\n--------------------\n"

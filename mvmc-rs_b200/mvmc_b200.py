@@ -24,7 +24,7 @@ EXPORTS = [
     "mvmc_b200_get_log_amplitudes", "mvmc_b200_stage_create", "mvmc_b200_stage_destroy",
     "mvmc_b200_stage_begin", "mvmc_b200_stage_propose_hop", "mvmc_b200_stage_accept_hop",
     "mvmc_b200_stage_propose_exchange", "mvmc_b200_stage_accept_exchange", "mvmc_b200_stage_recompute",
-    "mvmc_b200_stage_state",
+    "mvmc_b200_stage_state", "mvmc_b200_gram", "mvmc_b200_cholesky_solve",
 ]
 
 
@@ -104,6 +104,24 @@ def cg_solve_noalloc(samples_ptr, ns, na, mean_ptr, diag_ptr, g_ptr, inv_w, shif
         vp(samples_ptr), ctypes.c_longlong(ns), na, vp(mean_ptr), vp(diag_ptr), vp(g_ptr),
         ctypes.c_double(inv_w), ctypes.c_double(shift), ctypes.c_double(tol), max_iter, int(diag_scale),
         vp(x_ptr), vp(result_ptr), vp(stream)), "cg_solve_noalloc")
+
+
+def gram(store):
+    """out = Σ_s store[s] store[s]ᵀ for store of shape [samples, n] (device kernel)."""
+    store = np.ascontiguousarray(store, dtype=np.float64)
+    samples, n = store.shape
+    out = np.zeros((n, n))
+    _check(lib().mvmc_b200_gram(_ptr(store), n, ctypes.c_longlong(samples), _ptr(out)), "gram")
+    return out
+
+
+def cholesky_solve(s, rhs):
+    """Solve S x = rhs (S symmetric positive definite) on the device; returns (status, x)
+    with status 1 for a failed factorisation."""
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    x = np.ascontiguousarray(rhs, dtype=np.float64).copy()
+    rc = _check(lib().mvmc_b200_cholesky_solve(_ptr(s), _ptr(x), len(x)), "cholesky_solve")
+    return rc, x
 
 
 def default_options(**kw):

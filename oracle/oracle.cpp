@@ -1106,6 +1106,112 @@ int stochastic_opt_cg(Model& m, const Accum& tot, const std::vector<const Accum*
   return 0;
 }
 
+// Direct SR (NSRCG = 0; sr.rs:77-160, stochastic_opt_real_with_sr_info_timed): the Gram
+// OO = Σ_s O_s O_sᵀ / Wc of the stored rows (finalize_oo_store_real + c_order_gram_real,
+// sample order here), the active set by the redundancy cut on ⟨O²⟩ − ⟨O⟩²
+// (collect_active_real), S_ij = OO_ij − OO_0i OO_0j with the diagonal × (1 + DSROptStaDel)
+// and g_i = −2Δt (HO_i − HO_0 OO_0i) (sr_backend.rs:484-511), then the Cholesky solve
+// (LAPACK dpotrf('U') + dpotrs, sr.rs:535) and the update x_pi += x_si.
+int cholesky_solve_upper(std::vector<double>& a, std::vector<double>& b, int n) {
+  // a: row-major symmetric; U stored in the upper triangle, a = Uᵀ U
+  for (int j = 0; j < n; ++j) {
+    double d = a[static_cast<size_t>(j) * n + j];
+    for (int k = 0; k < j; ++k) d -= a[static_cast<size_t>(k) * n + j] * a[static_cast<size_t>(k) * n + j];
+    if (!(d > 0.0) || !std::isfinite(d)) return j + 1;
+    const double ujj = std::sqrt(d);
+    a[static_cast<size_t>(j) * n + j] = ujj;
+    for (int i = j + 1; i < n; ++i) {
+      double t = a[static_cast<size_t>(j) * n + i];
+      for (int k = 0; k < j; ++k) t -= a[static_cast<size_t>(k) * n + j] * a[static_cast<size_t>(k) * n + i];
+      a[static_cast<size_t>(j) * n + i] = t / ujj;
+    }
+  }
+  for (int i = 0; i < n; ++i) {  // Uᵀ y = b
+    double t = b[i];
+    for (int k = 0; k < i; ++k) t -= a[static_cast<size_t>(k) * n + i] * b[k];
+    b[i] = t / a[static_cast<size_t>(i) * n + i];
+  }
+  for (int i = n - 1; i >= 0; --i) {  // U x = y
+    double t = b[i];
+    for (int k = i + 1; k < n; ++k) t -= a[static_cast<size_t>(i) * n + k] * b[k];
+    b[i] = t / a[static_cast<size_t>(i) * n + i];
+  }
+  for (double v : b)
+    if (!std::isfinite(v)) return -1;
+  return 0;
+}
+
+int stochastic_opt_direct(Model& m, const Accum& tot, const std::vector<const Accum*>& walkers,
+                          mvmc::SrInfoRow* row, bool* wrote_row) {
+  *wrote_row = false;
+  const int size = m.sr_size(), npara = m.npara();
+  if (m.rescale_smat) throw std::runtime_error("RescaleSmat is outside the oracle's scope");
+  std::vector<double> oo(static_cast<size_t>(size) * size, 0.0);
+  const int nsamp = m.nvmc_sample;
+  for (const Accum* a : walkers)
+    for (int smp = 0; smp < nsamp; ++smp) {
+      const double* o = a->store.data() + static_cast<size_t>(smp) * size;
+      for (int i = 0; i < size; ++i)
+        for (int j = 0; j < size; ++j) oo[static_cast<size_t>(i) * size + j] += o[i] * o[j];
+    }
+  const double inv = 1.0 / tot.wc;
+  for (double& v : oo) v *= inv;
+  std::vector<double> s_diag(npara);
+  for (int pi = 0; pi < npara; ++pi)
+    s_diag[pi] = oo[static_cast<size_t>(pi + 1) * size + pi + 1] - oo[pi + 1] * oo[pi + 1];
+  bool any_nan = false;
+  double vmax = 0.0;
+  for (double v : s_diag) {
+    if (std::isnan(v)) any_nan = true;
+    vmax = std::fmax(vmax, v);
+  }
+  if (any_nan) vmax = NAN;
+  const double cut = vmax * m.red_cut;
+  auto optimised = [&](int c) { return static_cast<size_t>(c) < m.opt_flags.size() && m.opt_flags[c] == 1; };
+  std::vector<int> mapping;
+  for (int pi = 0; pi < npara; ++pi) {
+    if (!optimised(2 * pi)) continue;
+    if (s_diag[pi] < cut) continue;
+    mapping.push_back(pi);
+  }
+  if (mapping.empty()) return 0;
+  const int na = static_cast<int>(mapping.size());
+  std::vector<double> smat(static_cast<size_t>(na) * na), g(na);
+  for (int si = 0; si < na; ++si) {
+    const int pi = mapping[si] + 1;
+    for (int sj = 0; sj < na; ++sj) {
+      const int pj = mapping[sj] + 1;
+      double v = oo[static_cast<size_t>(pi) * size + pj] - oo[pi] * oo[pj];
+      if (si == sj) v *= 1.0 + m.sta_del;
+      smat[static_cast<size_t>(si) * na + sj] = v;
+    }
+    g[si] = -2.0 * m.step_dt * (tot.ho[pi] - tot.ho[0] * oo[pi]);
+  }
+  if (cholesky_solve_upper(smat, g, na) != 0) return 1;
+  // SRinfo in the complex index space of C (real value, zero imaginary variance)
+  double smax = s_diag[0], smin = s_diag[0];
+  int opt_num = 0, cut_num = 0;
+  for (int c = 0; c < 2 * npara; ++c) {
+    const double d = (c & 1) ? 0.0 : s_diag[c / 2];
+    if (d > smax) smax = d;
+    if (d < smin) smin = d;
+  }
+  for (int c = 0; c < 2 * npara; ++c) {
+    const double d = (c & 1) ? 0.0 : s_diag[c / 2];
+    if (!optimised(c)) ++opt_num;
+    else if (d < smax * m.red_cut) ++cut_num;
+  }
+  int imax = 0;
+  for (int i = 1; i < na; ++i)
+    if (std::fabs(g[imax]) < std::fabs(g[i])) imax = i;
+  *row = {npara, na, opt_num, cut_num, smax, smin, g[imax], 2 * mapping[imax], 0};
+  *wrote_row = true;
+  std::vector<double> p = mvmc::all_parameters(m);
+  for (int si = 0; si < na; ++si) p[mapping[si]] += g[si];
+  mvmc::set_all_parameters(m, p);
+  return 0;
+}
+
 // ===================================================================================
 // Drivers
 // ===================================================================================
@@ -1222,7 +1328,6 @@ int oracle_run_opt(const char* namelist, const char* initial_def, const char* ou
       m.nsr_opt_itr_step = nsteps;
       m.nsr_opt_itr_smp = std::min(m.nsr_opt_itr_smp, nsteps);
     }
-    if (m.nsrcg == 0) throw std::runtime_error("direct SR (NSRCG=0) is not covered; set NSRCG 1");
     const long long base = seed_override >= 0 ? seed_override : m.rnd_seed;
     std::vector<orc::Walker> ws(std::max(1, walkers));
     orc::seed_walkers(m, ws, base);
@@ -1245,7 +1350,8 @@ int oracle_run_opt(const char* namelist, const char* initial_def, const char* ou
       for (const auto& a : acc) ptrs.push_back(&a);
       mvmc::SrInfoRow row;
       bool wrote = false;
-      const int info = orc::stochastic_opt_cg(m, tot, ptrs, &row, &wrote);
+      const int info = m.nsrcg != 0 ? orc::stochastic_opt_cg(m, tot, ptrs, &row, &wrote)
+                                    : orc::stochastic_opt_direct(m, tot, ptrs, &row, &wrote);
       if (wrote) {
         mvmc::write_srinfo_row(out_dir, m, first_info, row);
         first_info = false;
@@ -1373,6 +1479,14 @@ int oracle_opt_step1_walkers(const char* namelist, const char* initial_def, int 
     orc::copy_err(e, err, err_len);
     return 1;
   }
+}
+
+int oracle_cholesky_solve(double* a, double* b, int n) {
+  std::vector<double> av(a, a + static_cast<size_t>(n) * n), bv(b, b + n);
+  const int info = orc::cholesky_solve_upper(av, bv, n);
+  std::copy(av.begin(), av.end(), a);
+  std::copy(bv.begin(), bv.end(), b);
+  return info;
 }
 
 void oracle_set_refresh_guard(double g) { orc::g_guard = g; }

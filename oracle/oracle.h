@@ -84,6 +84,11 @@ double oracle_refresh_drift(int reset);
 void oracle_set_refresh_guard(double g);
 void oracle_refresh_counts(long long* sched, long long* guard, int reset);
 
+// The direct SR solve (LAPACK dpotrf('U') + dpotrs order): a is n×n row-major symmetric,
+// overwritten by U (a = UᵀU) in its upper triangle; b becomes x. Returns 0, the 1-based
+// failing pivot, or -1 for a non-finite solution.
+int oracle_cholesky_solve(double* a, double* b, int n);
+
 // Model dimensions for buffer sizing: [nsite, ne, nqp, nproj, npara, nvmc_sample,
 // data_qty_smp, n_orb].
 int oracle_model_dims(const char* namelist, int* dims, char* err, int err_len);

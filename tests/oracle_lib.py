@@ -138,3 +138,10 @@ def stage_replay(namelist, params, idx0, ops, idx_seq, nqp, n):
     if rc != 0:
         raise RuntimeError(err.value.decode())
     return out, inv.reshape(nqp, n, n)
+
+
+def cholesky_solve(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64).copy()
+    b = np.ascontiguousarray(b, dtype=np.float64).copy()
+    info = lib().oracle_cholesky_solve(ptr(a), ptr(b), len(b))
+    return info, b

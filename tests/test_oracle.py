@@ -134,3 +134,29 @@ def test_cg_recurrence_matches_native_c(name, diag_scale):
         assert st == status, limit
         if limit <= 5:
             assert np.allclose(x, x_ref, rtol=1e-8, atol=1e-12 * np.abs(x_ref).max()), limit
+
+
+def test_cholesky_solve_matches_numpy_and_reports_pivot():
+    rng = np.random.default_rng(4)
+    m = rng.normal(size=(40, 40))
+    a = m @ m.T + 40 * np.eye(40)
+    b = rng.normal(size=40)
+    info, x = ol.cholesky_solve(a, b)
+    assert info == 0
+    assert np.allclose(x, np.linalg.solve(a, b), rtol=1e-12, atol=1e-14)
+    bad = a.copy()
+    bad[5, 5] = -1.0
+    info, _ = ol.cholesky_solve(bad, b)
+    assert info == 6
+
+
+def test_direct_sr_optimisation_runs_and_updates(tmp_path):
+    """NSRCG 0 (the reference example's default): Gram, redundancy cut, S and g, the
+    Cholesky solve and the update over three steps; SRinfo rows carry no info column."""
+    nl = os.path.join(G, "sr_operands_hubbard", "inputs", "namelist.def")
+    ol.run_opt(nl, str(tmp_path), walkers=2, nsteps=3, seed=3)
+    rows = np.loadtxt(tmp_path / "zvo_out.dat")
+    assert rows.shape[0] == 3 and np.all(np.isfinite(rows))
+    info = open(tmp_path / "zvo_SRinfo.dat").read().splitlines()
+    assert info[0].split()[-1] == "imax"
+    assert len(info) == 4 and all(len(r.split()) == 8 for r in info[1:])

@@ -1,8 +1,9 @@
 // K1: batched skew Pfaffian + inverse (PfaffianStages::pfaffian_inverse_batch).
 //
-// One CTA per plane. Planes up to the shared-memory limit are swept in shared memory
-// (row stride n+1 to spread banks); larger FP64 planes are swept in place in the output
-// buffer (L2-resident working set). Input and output are column-major as in
+// One CTA per plane. Planes with n ≤ 128 are swept in registers (k_pfinv_reg); larger
+// planes up to the shared-memory limit are swept in shared memory (ping-pong, or row stride
+// n+1 to spread banks); larger FP64 planes are swept in place in the output buffer
+// (L2-resident working set). Input and output are column-major as in
 // crates/mvmc-core/src/stage_backend.rs:121-165; the returned inverse is the true X⁻¹.
 #include <cuda_runtime.h>
 
@@ -114,6 +115,234 @@ int dispatch_pfinv_pp(const double* x, const int* sizes, const long long* offset
   return launch_pfinv_pp<T, 8>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
 }
 
+// Register-resident sweep for n ≤ G·R: thread (tr, tc) of a G×G block owns the R×R
+// elements (tr + G·a, tc + G·b) in registers, so every element update is two FMAs on
+// registers. A pivot step needs only rows p and q: the G threads holding the next pivot
+// row p publish it in shared memory together with its pivot search (first maximum of
+// |A[p][j]| over unswept j, a shuffle reduction inside their warp), the pivot A[p][q], its
+// reciprocal and the parity increment; the threads holding row q publish it after the
+// first barrier. Two barriers per pivot; buffers are double-buffered by step parity; the
+// swept set is a 128-bit mask kept identically by every thread.
+template <typename T, int G, int R>
+__global__ void __launch_bounds__(G * G, (G == 16 ? (sizeof(T) == 8 ? 3 : 4) : 1))
+    k_pfinv_reg(const double* __restrict__ x, const int* __restrict__ sizes,
+                const long long* __restrict__ offsets, int n_uniform, int planes, int n_max,
+                double* __restrict__ pf, double* __restrict__ inv, int* __restrict__ status) {
+  static_assert(G * R <= 128, "the swept mask holds 128 indices");
+  static_assert(G == 16 || G == 32, "a thread row is a half warp or a warp");
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* stage = reinterpret_cast<T*>(smem);                         // [n][n + 1]
+  T* rows = stage + static_cast<size_t>(n_max) * (n_max + 1);  // rowp[2][n_max], rowq[2][n_max]
+  __shared__ int s_q[2], s_par[2];
+  __shared__ T s_av[2], s_ia[2];
+  const int tid = threadIdx.x, nt = blockDim.x, tr = tid / G, tc = tid % G;
+  const unsigned segmask = G == 32 ? 0xffffffffu : (0xffffu << (tid & 16));
+  for (int plane = blockIdx.x; plane < planes; plane += gridDim.x) {
+    const int n = sizes ? sizes[plane] : n_uniform;
+    const long long off = offsets ? offsets[plane] : static_cast<long long>(plane) * n * n;
+    const double* xp = x + off;
+    double* ip = inv + off;
+    const int lda = n + 1;
+    {
+      int i = tid / n, j = tid - (tid / n) * n;
+      const int di = nt / n, dj = nt - (nt / n) * n;
+      for (int k = tid; k < n * n; k += nt) {
+        stage[i * lda + j] = static_cast<T>(-xp[k]);
+        i += di;
+        j += dj;
+        if (j >= n) {
+          j -= n;
+          ++i;
+        }
+      }
+    }
+    __syncthreads();
+    T e[R][R];
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = 0; b < R; ++b) {
+        const int i = tr + G * a, j = tc + G * b;
+        e[a][b] = (i < n && j < n) ? stage[i * lda + j] : T(0);
+      }
+    unsigned long long sw0 = 0ull, sw1 = 0ull;  // swept indices 0..63, 64..127
+    auto is_swept = [&](int j) { return ((j < 64 ? sw0 >> j : sw1 >> (j - 64)) & 1ull) != 0ull; };
+    // the threads holding row r publish it into buffer buf with its pivot search
+    auto publish = [&](int r, int buf) {
+      const int ar = r / G;
+      T* dst = rows + buf * n_max;
+      double best = -1.0;
+      int bi = n;
+      T bval = T(0);
+#pragma unroll
+      for (int a = 0; a < R; ++a) {
+        if (a != ar) continue;
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+          const int j = tc + G * b;
+          if (j >= n) continue;
+          dst[j] = e[a][b];
+          if (j != r && !is_swept(j)) {
+            const double v = fabs(static_cast<double>(e[a][b]));
+            if (v > best) {
+              best = v;
+              bi = j;
+              bval = e[a][b];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(segmask, best, o);
+        const int oi = __shfl_xor_sync(segmask, bi, o);
+        const T oval = __shfl_xor_sync(segmask, bval, o);
+        if (ov > best || (ov == best && oi < bi)) {
+          best = ov;
+          bi = oi;
+          bval = oval;
+        }
+      }
+      if (tc == 0) {
+        const bool ok = best > 0.0;
+        s_q[buf] = ok ? bi : n;
+        s_av[buf] = bval;
+        s_ia[buf] = ok ? T(1) / bval : T(0);
+        int cnt = 0;  // unswept indices strictly between r and q
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+          const int lo = max(r + 1, 64 * w), hi = min(bi, 64 * w + 64);
+          if (ok && lo < hi) {
+            const int len = hi - lo;
+            const unsigned long long range = (len == 64 ? ~0ull : ((1ull << len) - 1ull)) << (lo - 64 * w);
+            cnt += __popcll(~(w == 0 ? sw0 : sw1) & range);
+          }
+        }
+        s_par[buf] = cnt;
+      }
+    };
+    if (tr == 0) publish(0, 0);
+    int p = 0, parity = 0, st = 0;
+    double pfv = 1.0;
+    for (int k = 0; k < n / 2; ++k) {
+      const int par = k & 1;
+      const T* rp = rows + par * n_max;
+      T* rq = rows + (2 + par) * n_max;
+      __syncthreads();  // row p and its pivot published
+      const int q = s_q[par];
+      if (q >= n) {
+        st = p + 1;
+        break;
+      }
+      const T av = s_av[par], ia = s_ia[par];
+      parity += s_par[par];
+      pfv *= static_cast<double>(av);
+      if (tr == q % G) {
+        const int aq = q / G;
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+          if (a != aq) continue;
+#pragma unroll
+          for (int b = 0; b < R; ++b) {
+            const int j = tc + G * b;
+            if (j < n) rq[j] = e[a][b];
+          }
+        }
+      }
+      __syncthreads();  // row q published
+      // rank-2 update of every element (rows and columns p, q are overwritten below)
+      T rpj[R], rqj[R];
+#pragma unroll
+      for (int b = 0; b < R; ++b) {
+        const int j = tc + G * b;
+        rpj[b] = j < n ? rp[j] : T(0);
+        rqj[b] = j < n ? rq[j] : T(0);
+      }
+#pragma unroll
+      for (int a = 0; a < R; ++a) {
+        const int i = tr + G * a;
+        const T rpi = i < n ? rp[i] * ia : T(0), rqi = i < n ? rq[i] * ia : T(0);
+#pragma unroll
+        for (int b = 0; b < R; ++b) e[a][b] += rqi * rpj[b] - rpi * rqj[b];
+      }
+      // columns p, q: A[i][p] = −rq[i]/a, A[i][q] = rp[i]/a; then rows p, q (they take
+      // precedence): A[p][j] = rq[j]/a, A[q][j] = −rp[j]/a, A[p][q] = −1/a, A[q][p] = 1/a,
+      // A[p][p] = A[q][q] = 0. Only the threads holding those rows or columns take part.
+      if (tc == p % G || tc == q % G) {
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+          const int j = tc + G * b;
+          if (j != p && j != q) continue;
+#pragma unroll
+          for (int a = 0; a < R; ++a) {
+            const int i = tr + G * a;
+            if (i < n) e[a][b] = j == p ? -rq[i] * ia : rp[i] * ia;
+          }
+        }
+      }
+      if (tr == p % G || tr == q % G) {
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+          const int i = tr + G * a;
+          if (i != p && i != q) continue;
+#pragma unroll
+          for (int b = 0; b < R; ++b) {
+            const int j = tc + G * b;
+            if (i == p) e[a][b] = (j == q) ? -ia : (j == p ? T(0) : rqj[b] * ia);
+            else e[a][b] = (j == p) ? ia : (j == q ? T(0) : -rpj[b] * ia);
+          }
+        }
+      }
+      if (p < 64) sw0 |= 1ull << p;
+      else sw1 |= 1ull << (p - 64);
+      if (q < 64) sw0 |= 1ull << q;
+      else sw1 |= 1ull << (q - 64);
+      int np = n;
+      if (~sw0) np = min(n, __ffsll(static_cast<long long>(~sw0)) - 1);
+      else if (~sw1) np = min(n, 64 + __ffsll(static_cast<long long>(~sw1)) - 1);
+      if (np < n && tr == np % G) publish(np, 1 - par);
+      p = np < n ? np : 0;
+    }
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = 0; b < R; ++b) {
+        const int i = tr + G * a, j = tc + G * b;
+        if (i < n && j < n) ip[static_cast<size_t>(i) * n + j] = -static_cast<double>(e[a][b]);
+      }
+    if (tid == 0) {
+      double v = (parity & 1) ? -pfv : pfv;
+      if (st == 0 && !isfinite(v)) st = -1;
+      if (st != 0) v = 0.0;
+      pf[plane] = v;
+      status[plane] = st;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, int G, int R>
+int launch_pfinv_reg(const double* x, const int* sizes, const long long* offsets, int n_uniform, int planes,
+                     int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
+  const size_t smem = sizeof(T) * (static_cast<size_t>(n_max) * (n_max + 1) + 4 * static_cast<size_t>(n_max));
+  auto kernel = k_pfinv_reg<T, G, R>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 0;
+  MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G * G, smem));
+  const int grid = std::max(1, std::min(planes, std::max(1, per_sm) * device_sm_count()));
+  kernel<<<grid, G * G, smem, stream>>>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+template <typename T>
+int dispatch_pfinv_reg(const double* x, const int* sizes, const long long* offsets, int n_uniform, int planes,
+                       int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
+  if (n_max <= 32) return launch_pfinv_reg<T, 16, 2>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  if (n_max <= 64) return launch_pfinv_reg<T, 16, 4>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  return launch_pfinv_reg<T, 32, 4>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+}
+
 template <typename T>
 size_t pfinv_smem_bytes(int n_max, bool smem_matrix) {
   size_t b = (gj_shared_bytes<T>(n_max) + 15) & ~size_t(15);
@@ -164,6 +393,11 @@ int pfinv_device(const double* x, const int* sizes, const long long* offsets, in
   if (planes <= 0) return kOk;
   if (n_max <= 0 || (n_max & 1) || !x || !pf || !inv || !status) return kErrArgument;
   const int limit = device_smem_limit();
+  if (n_max <= 128 && (precision == 32 || precision == 64)) {
+    if (precision == 32)
+      return dispatch_pfinv_reg<float>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+    return dispatch_pfinv_reg<double>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  }
   const size_t pp_bytes = 2 * static_cast<size_t>(n_max) * n_max * (precision == 32 ? 4 : 8);
   if (n_max <= 256 && pp_bytes <= static_cast<size_t>(limit)) {
     if (precision == 32)

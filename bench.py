@@ -16,8 +16,10 @@ Pfaffian workloads (pfinv64, pfinv_mix): a step is one batched Pfaffian + invers
 over B = 8192 (8190 for the five-size mix) seeded skew planes; `value` is planes/s.
 
 `e2e` times the same steps through the public C ABI calls with host buffers, host↔device
-copies inside the timed region. For N > 1 (torchrun) every rank runs its own walker
-ensemble (seeds offset by rank × walkers): replicas, no data-path collective.
+copies inside the timed region. For N > 1 (torchrun) every rank samples and measures its
+own walker ensemble (seeds offset by rank × walkers, no collective on that path) and the
+SR step is sharded: the measurement sums and every CG product are added across ranks
+over NCCL (mvmc-rs_b200/sharded.py), so all ranks apply the same update.
 """
 import argparse
 import json
@@ -230,10 +232,25 @@ def time_engine(args, precision, W, namelist, initial_def, cfg, dims, rank, loca
                     refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision)
     stream = torch.cuda.ExternalStream(eng.stream())
     energy = None
+    if ws > 1:
+        # walker-sharded SR: the sums and every CG product are added across ranks (NCCL)
+        import sharded
+
+        def reduce(a):
+            t = torch.as_tensor(np.asarray(a, dtype=np.float64), device="cuda")
+            dist.all_reduce(t)
+            return t.cpu().numpy()
+
+        def sr_step():
+            info = sharded.sr_step(eng, reduce)
+            return 0, np.array([info[k] for k in ("npara", "nsmat", "opt_cut", "diag_cut", "sdiag_max",
+                                                  "sdiag_min", "rmax", "imax", "info")], dtype=np.float64)
+    else:
+        sr_step = eng.sr_cg
     for _ in range(args.warmup):
         eng.sample()
         eng.measure()
-        eng.sr_cg()
+        sr_step()
     torch.cuda.synchronize()
     if timed_hook:
         timed_hook("start")
@@ -253,7 +270,7 @@ def time_engine(args, precision, W, namelist, initial_def, cfg, dims, rank, loca
         b.record(stream)
         e, ho, oo = eng.measure()
         c.record(stream)
-        rc, sri = eng.sr_cg()
+        rc, sri = sr_step()
         energy = float(e[1])
         cg_iters.append(int(sri[8]))
         marks.append((a, b, c))
@@ -363,7 +380,7 @@ def engine_bench(args, ws, rank, local):
         "dtype": "f64" if args.precision == 64 else "f32+f64refresh", "data": "synthetic",
         "config": {"workload": args.config, "walkers_per_gpu": W, "nsite": ns, "n": n, "nqp": nqp,
                    "npara": dims["npara"], "sweeps_per_walker_step": sweeps_per_walker_step,
-                   "precision": args.precision, "parallelism": f"replicas{ws}",
+                   "precision": args.precision, "parallelism": f"walker-sharded{ws}" if ws > 1 else "1",
                    "refresh_sweeps": args.refresh if args.precision == 32 else None,
                    "refresh_guard": args.guard if args.precision == 32 else None,
                    "sr_precision": args.sr_precision or 64, "sr": "direct" if args.direct else "cg",

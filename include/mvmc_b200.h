@@ -223,6 +223,30 @@ int mvmc_b200_gram(const double* store, int n, long long samples, double* out);
  * 0 on success. The engine's direct SR (NSRCG 0) runs the same kernels on device buffers. */
 int mvmc_b200_cholesky_solve(const double* s, double* rhs, int n);
 
+/* ---------------------------------------------------------------------------------
+ * Walker-sharded SR across ranks (the reference's Reducer seam, reducer.rs:20-168, and
+ * stochastic_opt_cg_with_reducer, sr_cg.rs:201-490): each rank samples and measures its
+ * own walkers; the caller adds the measurement sums and every CG product across ranks,
+ * runs the recurrence, and every rank applies the same update (mvmc-rs_b200/sharded.py).
+ * ------------------------------------------------------------------------------- */
+/* Sums of the last measurement over this context's walkers, before the weight average:
+ * sums[5 + 3*sr_size] = {Wc, Σ E, Σ E², Σ Sz, Σ Sz², Σ HO[sr_size], Σ O[sr_size],
+ * Σ O²[sr_size]}. */
+int mvmc_b200_measure_sums(const mvmc_b200_ctx* ctx, double* sums);
+/* Compact the active columns map[0..na) (parameter indices) of the stored O rows. */
+int mvmc_b200_sr_gather(mvmc_b200_ctx* ctx, const int* map, int na);
+/* SrStages::cg_local_product (sr_backend.rs:249-255): z = Σ_s O_s (O_s·v) over this
+ * context's samples and the gathered columns; no mean, diagonal or cross-rank terms.
+ * v, z: na host doubles. */
+int mvmc_b200_sr_local_product(mvmc_b200_ctx* ctx, const double* v, double* z);
+/* Apply an SR solution: parameter map[i] += x[i], then sync_modified_parameter and the
+ * upload (update_parameter_value, sr.rs:439; sync.rs:87). */
+int mvmc_b200_sr_apply(mvmc_b200_ctx* ctx, const int* map, int na, const double* x);
+/* SR settings: cfg[10] = {NSRCG, DSROptRedCut, DSROptStepDt, DSROptStaDel, DSROptCGTol,
+ * NSROptCGMaxIter, DiagScale, CG fallback, CG abort-on-fail, NPara}; flags[2*NPara] the
+ * optimisation flags (real, imaginary) per parameter (may be NULL). */
+int mvmc_b200_sr_config(const mvmc_b200_ctx* ctx, double* cfg, int* flags);
+
 /* The context's CUDA stream (a cudaStream_t), for timing and ordering with caller work. */
 void* mvmc_b200_stream(mvmc_b200_ctx* ctx);
 

@@ -41,6 +41,9 @@ int launch_gram(const double* store, int n, long long ns, double inv_w, double* 
 int launch_assemble_s(const double* oo, int n, const int* map, int na, double ratio_diag, double* s,
                       cudaStream_t stream);
 int launch_cholesky_solve(double* a, int n, double* b, int* info_dev, cudaStream_t stream);
+int local_product_chunks(long long ns, int na);
+int launch_local_product(const double* oa, long long ns, int na, const double* v, double* z, double* y,
+                         double* part, cudaStream_t stream);
 
 // K0: SlaterElm[q][rs_i][rs_j] from the Slater parameters (update_slater_elm,
 // crates/mvmc-core/src/slater_update.rs:17-120).
@@ -128,6 +131,12 @@ struct mvmc_b200_ctx {
   double* d_smat = nullptr;
   size_t smat_cap = 0;
   int* d_info = nullptr;
+  // walker-sharded SR: compact active columns and the product buffers
+  int shard_na = 0;
+  double* d_shard_vec = nullptr;  // v, z (2·na)
+  size_t shard_vec_cap = 0;
+  double* d_shard_part = nullptr;
+  size_t shard_part_cap = 0;
   std::vector<double> tot;  // host copy of the last reduction
   long long h2d = 0, d2h = 0;  // bytes copied across the host boundary
   bool sampled = false, measured = false;
@@ -1058,4 +1067,106 @@ extern "C" int mvmc_b200_stage_state(const mvmc_b200_stage* st, double* pf, doub
       check(cudaMemcpy(inv_m, st->b.planes, sizeof(double) * nn * c->dm.nqp, cudaMemcpyDeviceToHost), "stage inv");
     return MVMC_B200_OK;
   });
+}
+
+// ---------------------------------------------------------------------------------------
+// Walker-sharded SR (the reference's Reducer seam, crates/mvmc-core/src/reducer.rs:20-168):
+// each rank measures its own walkers; the caller adds the sums and the CG products across
+// ranks and runs the recurrence; every rank applies the same update.
+// ---------------------------------------------------------------------------------------
+extern "C" int mvmc_b200_measure_sums(const mvmc_b200_ctx* c, double* sums) {
+  if (!c || !sums) return MVMC_B200_EARG;
+  if (!c->measured) return MVMC_B200_ESTATE;
+  const double wc = c->tot[0];
+  sums[0] = wc;
+  for (size_t k = 1; k < c->tot.size(); ++k) sums[k] = c->tot[k] * wc;
+  return MVMC_B200_OK;
+}
+
+extern "C" int mvmc_b200_sr_gather(mvmc_b200_ctx* c, const int* map, int na) {
+  if (!c || !map || na <= 0) return MVMC_B200_EARG;
+  if (!c->measured) return MVMC_B200_ESTATE;
+  const int npara = c->m.npara();
+  for (int i = 0; i < na; ++i)
+    if (map[i] < 0 || map[i] >= npara) return MVMC_B200_EARG;
+  return guarded([&]() {
+    const long long ns = static_cast<long long>(c->W) * c->S;
+    if (static_cast<size_t>(ns) * na > c->oa_cap) {
+      c->d_oa = c->alloc<double>(static_cast<size_t>(ns) * na);
+      c->oa_cap = static_cast<size_t>(ns) * na;
+    }
+    if (static_cast<size_t>(ns) > c->y_cap) {
+      c->d_y = c->alloc<double>(ns);
+      c->y_cap = static_cast<size_t>(ns);
+    }
+    if (static_cast<size_t>(na) > c->map_cap) {
+      c->d_map = c->alloc<int>(na);
+      c->map_cap = na;
+    }
+    if (static_cast<size_t>(2) * na > c->shard_vec_cap) {
+      c->d_shard_vec = c->alloc<double>(static_cast<size_t>(2) * na);
+      c->shard_vec_cap = static_cast<size_t>(2) * na;
+    }
+    const size_t part = static_cast<size_t>(local_product_chunks(ns, na)) * na;
+    if (part > c->shard_part_cap) {
+      c->d_shard_part = c->alloc<double>(part);
+      c->shard_part_cap = part;
+    }
+    check(cudaMemcpyAsync(c->d_map, map, sizeof(int) * na, cudaMemcpyHostToDevice, c->stream), "upload map");
+    c->h2d += static_cast<long long>(sizeof(int) * na);
+    const int rc = launch_gather_active(c->d_ostore, c->dm.sr_size, ns, c->d_map, na, c->d_oa, c->stream);
+    if (rc != kOk) return rc;
+    check(cudaStreamSynchronize(c->stream), "gather");
+    c->shard_na = na;
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_sr_local_product(mvmc_b200_ctx* c, const double* v, double* z) {
+  if (!c || !v || !z) return MVMC_B200_EARG;
+  if (c->shard_na <= 0) return MVMC_B200_ESTATE;
+  return guarded([&]() {
+    const int na = c->shard_na;
+    const long long ns = static_cast<long long>(c->W) * c->S;
+    double* dv = c->d_shard_vec;
+    double* dz = dv + na;
+    check(cudaMemcpyAsync(dv, v, sizeof(double) * na, cudaMemcpyHostToDevice, c->stream), "upload v");
+    const int rc = launch_local_product(c->d_oa, ns, na, dv, dz, c->d_y, c->d_shard_part, c->stream);
+    if (rc != kOk) return rc;
+    check(cudaMemcpyAsync(z, dz, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download z");
+    check(cudaStreamSynchronize(c->stream), "local product");
+    c->h2d += static_cast<long long>(sizeof(double) * na);
+    c->d2h += static_cast<long long>(sizeof(double) * na);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_sr_apply(mvmc_b200_ctx* c, const int* map, int na, const double* x) {
+  if (!c || (na > 0 && (!map || !x)) || na < 0) return MVMC_B200_EARG;
+  const int npara = c->m.npara();
+  for (int i = 0; i < na; ++i)
+    if (map[i] < 0 || map[i] >= npara) return MVMC_B200_EARG;
+  return guarded([&]() {
+    std::vector<double> p = mvmc::all_parameters(c->m);
+    for (int si = 0; si < na; ++si) p[map[si]] += x[si];
+    mvmc::set_all_parameters(c->m, p);
+    mvmc::sync_modified_parameter(c->m, true);
+    upload_parameters(c);
+    check(cudaStreamSynchronize(c->stream), "apply");
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_sr_config(const mvmc_b200_ctx* c, double* cfg, int* flags) {
+  if (!c || !cfg) return MVMC_B200_EARG;
+  const mvmc::Model& m = c->m;
+  const double v[10] = {static_cast<double>(m.nsrcg), m.red_cut, m.step_dt, m.sta_del, m.cg_tol,
+                        static_cast<double>(m.cg_max_iter), m.diag_scale ? 1.0 : 0.0, m.cg_fallback ? 1.0 : 0.0,
+                        m.cg_abort ? 1.0 : 0.0, static_cast<double>(m.npara())};
+  std::copy(v, v + 10, cfg);
+  if (flags) {
+    const int width = 2 * m.npara();
+    for (int k = 0; k < width; ++k) flags[k] = static_cast<size_t>(k) < m.opt_flags.size() ? m.opt_flags[k] : 0;
+  }
+  return MVMC_B200_OK;
 }

@@ -323,6 +323,63 @@ int launch_gather_active(const double* store, int sr_size, long long ns, const i
   return kOk;
 }
 
+// Local sampled product of a rank's samples (SrStages::cg_local_product,
+// sr_backend.rs:249-255): z = Σ_s O_s (O_s · v), no mean, diagonal or cross-rank terms.
+// y[s] = O_s·v by one warp per row; per-chunk column sums; the chunks added in order.
+__global__ void k_local_rowdot(const double* __restrict__ oa, long long ns, int na, const double* __restrict__ v,
+                               double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  for (long long s = gw; s < ns; s += nw) {
+    double t = 0.0;
+    for (int i = lane; i < na; i += 32) t += oa[s * na + i] * v[i];
+    t = warp_sum(t);
+    if (lane == 0) y[s] = t;
+  }
+}
+
+__global__ void k_local_colpart(const double* __restrict__ oa, long long ns, int na, const double* __restrict__ y,
+                                int nchunk, double* __restrict__ part) {
+  const int ntile = (na + blockDim.x - 1) / blockDim.x;
+  const long long chunk = (ns + nchunk - 1) / nchunk;
+  for (int item = blockIdx.x; item < ntile * nchunk; item += gridDim.x) {
+    const int tile = item % ntile, c = item / ntile;
+    const int i = tile * blockDim.x + threadIdx.x;
+    if (i >= na) continue;
+    const long long s0 = c * chunk, s1 = min(ns, s0 + chunk);
+    double t = 0.0;
+    for (long long s = s0; s < s1; ++s) t += oa[s * na + i] * y[s];
+    part[static_cast<long long>(c) * na + i] = t;
+  }
+}
+
+__global__ void k_local_colsum(const double* __restrict__ part, int nchunk, int na, double* __restrict__ z) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int c = 0; c < nchunk; ++c) t += part[static_cast<long long>(c) * na + i];
+    z[i] = t;
+  }
+}
+
+int local_product_chunks(long long ns, int na) {
+  const int ntile = (na + 255) / 256;
+  return static_cast<int>(std::max<long long>(1, std::min<long long>(ns, std::max(1, 592 / ntile))));
+}
+
+// y: ns doubles, part: local_product_chunks(ns, na)·na doubles (device).
+int launch_local_product(const double* oa, long long ns, int na, const double* v, double* z, double* y,
+                         double* part, cudaStream_t stream) {
+  const int nchunk = local_product_chunks(ns, na);
+  const int rows_grid = static_cast<int>(std::max<long long>(1, std::min<long long>((ns + 7) / 8, 148LL * 16)));
+  k_local_rowdot<<<rows_grid, 256, 0, stream>>>(oa, ns, na, v, y);
+  const int ntile = (na + 255) / 256;
+  k_local_colpart<<<std::max(1, std::min(ntile * nchunk, 148 * 8)), 256, 0, stream>>>(oa, ns, na, y, nchunk, part);
+  k_local_colsum<<<std::max(1, (na + 255) / 256), 256, 0, stream>>>(part, nchunk, na, z);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
 // One block per SM (co-resident for the cooperative launch).
 int cg_grid_blocks(long long ns, int na) {
   (void)ns;

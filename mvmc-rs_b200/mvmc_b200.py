@@ -25,6 +25,8 @@ EXPORTS = [
     "mvmc_b200_stage_begin", "mvmc_b200_stage_propose_hop", "mvmc_b200_stage_accept_hop",
     "mvmc_b200_stage_propose_exchange", "mvmc_b200_stage_accept_exchange", "mvmc_b200_stage_recompute",
     "mvmc_b200_stage_state", "mvmc_b200_gram", "mvmc_b200_cholesky_solve",
+    "mvmc_b200_measure_sums", "mvmc_b200_sr_gather", "mvmc_b200_sr_local_product", "mvmc_b200_sr_apply",
+    "mvmc_b200_sr_config",
 ]
 
 
@@ -210,6 +212,35 @@ class Engine:
         _check(lib().mvmc_b200_get_log_amplitudes(self.ctx, _ptr(out), ctypes.c_longlong(out.size)),
                "log_amplitudes")
         return out
+
+    def measure_sums(self):
+        """Sums of the last measurement before the weight average (Wc first)."""
+        out = np.zeros(5 + 3 * self.sr_size)
+        _check(lib().mvmc_b200_measure_sums(self.ctx, _ptr(out)), "measure_sums")
+        return out
+
+    def sr_gather(self, mapping):
+        m = np.ascontiguousarray(mapping, dtype=np.int32)
+        _check(lib().mvmc_b200_sr_gather(self.ctx, _ptr(m), len(m)), "sr_gather")
+
+    def sr_local_product(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        z = np.zeros_like(v)
+        _check(lib().mvmc_b200_sr_local_product(self.ctx, _ptr(v), _ptr(z)), "sr_local_product")
+        return z
+
+    def sr_apply(self, mapping, x):
+        m = np.ascontiguousarray(mapping, dtype=np.int32)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        _check(lib().mvmc_b200_sr_apply(self.ctx, _ptr(m), len(m), _ptr(x)), "sr_apply")
+
+    def sr_config(self):
+        cfg = np.zeros(10)
+        flags = np.zeros(2 * self.dims["npara"], dtype=np.int32)
+        _check(lib().mvmc_b200_sr_config(self.ctx, _ptr(cfg), _ptr(flags)), "sr_config")
+        keys = ["nsrcg", "red_cut", "step_dt", "sta_del", "cg_tol", "cg_max_iter", "diag_scale", "cg_fallback",
+                "cg_abort", "npara"]
+        return dict(zip(keys, cfg.tolist())), flags
 
     def sr_cg(self):
         info = np.zeros(9)

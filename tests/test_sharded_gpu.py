@@ -1,0 +1,38 @@
+"""The walker-sharded SR step (mvmc-rs_b200/sharded.py) on the device engine with one rank
+(identity reducer) against the engine's own SR-CG on the same samples."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from mvmc_lib import ROOT, lattice, mvmc
+
+sys.path.insert(0, os.path.join(ROOT, "mvmc-rs_b200"))
+import sharded  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def test_sharded_step_on_one_rank_matches_engine_sr(tmp_path):
+    lat = lattice()
+    cfg = dict(lat.CONFIGS["square8"])
+    cfg.update(interval=2, cg_tol=1e-9, cg_max_iter=1000)
+    nl, init, _ = lat.write_inputs(str(tmp_path / "in"), **cfg)
+    a = mvmc().Engine(nl, init, walkers=256, precision=64, seed=9)
+    b = mvmc().Engine(nl, init, walkers=256, precision=64, seed=9)
+    p0 = a.parameters()
+    for eng in (a, b):
+        eng.sample()
+        eng.measure()
+    # same chains; the O_k accumulation of the measurement uses shared-memory atomics, so the
+    # sums agree to rounding
+    assert np.allclose(a.measure_sums(), b.measure_sums(), rtol=1e-12, atol=1e-12)
+    rc, info = a.sr_cg()
+    sinfo = sharded.sr_step(b, lambda x: x)
+    assert rc == 0 and info[8] >= 0 and sinfo["info"] >= 0
+    assert sinfo["nsmat"] == int(info[1]) and sinfo["opt_cut"] == int(info[2]) and sinfo["diag_cut"] == int(info[3])
+    da, db = a.parameters() - p0, b.parameters() - p0
+    assert np.allclose(db, da, rtol=1e-6, atol=1e-6 * np.abs(da).max())
+    a.close()
+    b.close()

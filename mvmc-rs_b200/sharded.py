@@ -18,6 +18,12 @@ one rank; torch.distributed all_reduce over NCCL in bench.py, gloo in the tests)
 import numpy as np
 
 
+def _dot(a, b):
+    """Single-threaded pairwise sum: the same bits on every rank whatever the BLAS
+    threading, so every rank takes the same CG branch."""
+    return float(np.sum(a * b))
+
+
 def operands(sums):
     """Weight average of the reduced sums (weight_average_sr_opt_real, average.rs:50)."""
     size = (len(sums) - 5) // 3
@@ -68,10 +74,10 @@ def cg_solve(apply, g, diag, shift, tol, max_iter, diag_scale):
     if diag_scale:
         r = g - apply(x)
         d = precond(r)
-        delta = float(r @ d)
+        delta = _dot(r, d)
     else:
         d = g.copy()
-        delta = float(r @ r)
+        delta = _dot(r, r)
     status, it, done = 0, 0, False
     if not np.isfinite(delta):
         return x, -1
@@ -83,7 +89,7 @@ def cg_solve(apply, g, diag, shift, tol, max_iter, diag_scale):
         if abs(delta) < threshold:
             break
         q = apply(d)
-        dq = float(d @ q)
+        dq = _dot(d, q)
         if not np.isfinite(dq) or abs(dq) < 1e-20:
             status, done = failed, True
             break
@@ -98,9 +104,9 @@ def cg_solve(apply, g, diag, shift, tol, max_iter, diag_scale):
             r = r - alpha * q
         if diag_scale:
             q = precond(r)
-            delta_new = float(r @ q)
+            delta_new = _dot(r, q)
         else:
-            delta_new = float(r @ r)
+            delta_new = _dot(r, r)
         if not np.isfinite(delta_new) or abs(delta) < 1e-20:
             status, done = failed, True
             break
@@ -142,7 +148,7 @@ def sr_step(local, reduce):
 
     def apply(v):
         z = reduce(local.sr_local_product(v))
-        return inv_w * z - float(mean @ v) * mean + shift * diag * v
+        return inv_w * z - _dot(mean, v) * mean + shift * diag * v
 
     max_iter = int(cfg["cg_max_iter"]) if cfg["cg_max_iter"] > 0 else len(mapping)
     diag_scale = bool(cfg["diag_scale"])

@@ -54,7 +54,7 @@ __host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_p
 }
 
 template <int JPL, bool kSmemPlane>
-__global__ void __launch_bounds__(kMeasThreads)
+__global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
     k_measure(DevModel m, const int* __restrict__ s_idx, const int* __restrict__ s_cfg,
               const int* __restrict__ s_num, const int* __restrict__ s_cnt, int nsamples,
               double* __restrict__ gws, double* __restrict__ ostore, double* __restrict__ eloc,
@@ -125,7 +125,9 @@ __global__ void __launch_bounds__(kMeasThreads)
       __syncthreads();
       double pfv;
       int st;
-      gj_pfinv_pp<double, JPL, kSmemPlane ? 1 : 4>(A, Bpp, n, pfv, st);
+      // planes in L2: a few rows in flight per warp, fewer for wide rows so that two
+      // samples share an SM
+      gj_pfinv_pp<double, JPL, kSmemPlane ? 1 : (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, Bpp, n, pfv, st);
       if (st != 0) {
         if (tid == 0) s_bad = 1;
         __syncthreads();

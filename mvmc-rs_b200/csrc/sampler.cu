@@ -275,11 +275,46 @@ __device__ __forceinline__ void col_dot_pair(const T* __restrict__ P0, const T* 
   r1 = (b[0] + b[1]) + (b[2] + b[3]);
 }
 
-// out_k[q][j] = −Σ_i P_q[i][j]·vec[q][in][i] → vec[q][out], all (plane, column) items of
-// the CTA, two per thread where there are enough.
+// Column range [i0, i1) of col_dot.
+template <typename T>
+__device__ __forceinline__ T col_dot_range(const T* __restrict__ P, const T* __restrict__ v, int n, int i0,
+                                           int i1) {
+  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+  int i = i0;
+  for (; i + 4 <= i1; i += 4) {
+    a0 += P[(i + 0) * n] * v[i + 0];
+    a1 += P[(i + 1) * n] * v[i + 1];
+    a2 += P[(i + 2) * n] * v[i + 2];
+    a3 += P[(i + 3) * n] * v[i + 3];
+  }
+  for (; i < i1; ++i) a0 += P[i * n] * v[i];
+  return (a0 + a1) + (a2 + a3);
+}
+
+// out[q][j] = −Σ_i P_q[i][j]·vec[q][in][i] → vec[q][out] for every (plane, column), two
+// columns per thread where there are enough. With fewer columns than threads (one wide
+// plane) each column is split into two row halves on two threads, the second half
+// parked in slot 3 and added in order after a barrier. Ends without a barrier.
 template <typename T>
 __device__ __forceinline__ void planes_col_dot(const DevModel& m, const WalkerSmem<T>& s, int in, int out) {
   const int n = m.n, total = m.nqp * n, nt = blockDim.x;
+  if (total <= nt && out != 3 && in != 3) {
+    const int half = ((n + 1) / 2 + 3) & ~3;
+    for (int k = threadIdx.x; k < 2 * total; k += nt) {
+      const int seg = k / total, kk = k - seg * total;
+      const int q = kk / n, j = kk - q * n;
+      const T* P = s.planes + static_cast<size_t>(q) * n * n + j;
+      const int i0 = seg ? min(half, n) : 0, i1 = seg ? n : min(half, n);
+      const T r = col_dot_range(P, s.vec + (q * 4 + in) * n, n, i0, i1);
+      s.vec[(q * 4 + (seg ? 3 : out)) * n + j] = r;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < total; k += nt) {
+      const int q = k / n, j = k - q * n;
+      s.vec[(q * 4 + out) * n + j] = -(s.vec[(q * 4 + out) * n + j] + s.vec[(q * 4 + 3) * n + j]);
+    }
+    return;
+  }
   for (int k = threadIdx.x; k < total; k += 2 * nt) {
     const int q = k / n, j = k - q * n;
     const T* P = s.planes + static_cast<size_t>(q) * n * n + j;

@@ -299,6 +299,64 @@ Model read_expert(const std::string& namelist_path) {
   m.gutz.assign(m.n_gutz, 0.0);
   m.jast.assign(m.n_jast, 0.0);
   m.slater.assign(m.n_orb, 0.0);
+
+  // PhysCal Green-function lists (green.rs:16-270): the count on line 2, five header
+  // lines, one term per non-empty body line; sites in [0, Nsite), spins 0 or 1, and the
+  // number of rows equal to the count.
+  auto green_rows = [&](const char* key, size_t fields, bool exact) {
+    std::vector<std::vector<int>> rows;
+    if (!files.count(key)) return rows;
+    const std::string path = files[key];
+    auto lines = read_lines(path);
+    if (lines.size() < 2) throw std::runtime_error(path + ": missing count on line 2");
+    auto head = tokens(lines[1]);
+    if (head.size() < 2) throw std::runtime_error(path + ": missing count on line 2");
+    const int count = std::stoi(head[1]);
+    if (count == 0) return rows;
+    if (lines.size() < 5) throw std::runtime_error(path + ": fewer than five header lines");
+    for (size_t k = 5; k < lines.size(); ++k) {
+      auto t = tokens(lines[k]);
+      if (t.empty()) continue;
+      if (t.size() < fields || (exact && t.size() != fields))
+        throw std::runtime_error(path + ": expected " + std::to_string(fields) + " integer fields");
+      std::vector<int> row(fields);
+      for (size_t f = 0; f < fields; ++f) {
+        size_t used = 0;
+        row[f] = std::stoi(t[f], &used);
+        if (used != t[f].size()) throw std::runtime_error(path + ": malformed integer " + t[f]);
+        const bool spin = f % 2 == 1;
+        if (spin ? (row[f] != 0 && row[f] != 1) : (row[f] < 0 || row[f] >= ns))
+          throw std::runtime_error(path + ": site or spin out of range");
+      }
+      rows.push_back(row);
+    }
+    if (static_cast<int>(rows.size()) != count)
+      throw std::runtime_error(path + ": declared row count does not match the rows");
+    return rows;
+  };
+  for (const auto& r : green_rows("OneBodyG", 4, false)) m.green_one.push_back({r[0], r[1], r[2], r[3]});
+  for (const auto& r : green_rows("TwoBodyG", 8, false))
+    m.green_two.push_back({r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]});
+  // TwoBodyGEx "i s j t k u l v" is the product <c†_is c_jt>·<c†_lv c_ku>*: its factors are
+  // the one-body terms (i s j t) and (l v k u) (green.rs:252-261; types.rs:1169-1215).
+  const auto ex_rows = green_rows("TwoBodyGEx", 8, true);
+  if (!ex_rows.empty()) {
+    std::vector<GreenOneTerm> canonical;
+    for (const auto& t : m.green_one)
+      if (std::find(canonical.begin(), canonical.end(), t) == canonical.end()) canonical.push_back(t);
+    m.green_one = canonical;
+  }
+  auto one_index = [&](const GreenOneTerm& t) {
+    auto it = std::find(m.green_one.begin(), m.green_one.end(), t);
+    if (it != m.green_one.end()) return static_cast<int>(it - m.green_one.begin());
+    m.green_one.push_back(t);
+    return static_cast<int>(m.green_one.size()) - 1;
+  };
+  for (const auto& r : ex_rows) {
+    const int first = one_index({r[0], r[1], r[2], r[3]});
+    const int second = one_index({r[6], r[7], r[4], r[5]});
+    m.green_two_ex.emplace_back(first, second);
+  }
   return m;
 }
 
@@ -531,6 +589,58 @@ void write_out_row(const Model& m, const std::string& dir, int step, const StepE
     std::fprintf(v, "%s %s 0.0 ", c_double(p).c_str(), c_double(0.0).c_str());
   std::fprintf(v, "\n");
   std::fclose(v);
+}
+
+void write_physcal_block(const Model& m, const std::string& dir, int index, const StepEnergy& e,
+                         const double* one, const double* two_ex, const double* two) {
+  char tag[32];
+  std::snprintf(tag, sizeof tag, "_%03d.dat", index);
+  auto open = [&](const char* kind) {
+    const std::string path = dir + "/" + m.data_head + "_" + kind + tag;
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + path);
+    return f;
+  };
+  // C complex quotient (etot2 − etot²)/etot² with zero imaginary parts: a plain division.
+  const double variance = (e.etot2 - e.etot * e.etot) / (e.etot * e.etot);
+  FILE* f = open("out");
+  std::fprintf(f, "%s %s  %s %s %s %s\n", c_double(e.etot).c_str(), c_double(0.0).c_str(),
+               c_double(e.etot2).c_str(), c_double(variance).c_str(), c_double_nospace(e.sztot).c_str(),
+               c_double_nospace(e.sztot2).c_str());
+  std::fclose(f);
+  f = open("var");
+  std::fprintf(f, "%s %s 0.0 %s %s 0.0 ", c_double(e.etot).c_str(), c_double(0.0).c_str(),
+               c_double(e.etot2).c_str(), c_double(0.0).c_str());
+  for (double p : all_parameters(m)) std::fprintf(f, "%s %s 0.0 ", c_double(p).c_str(), c_double(0.0).c_str());
+  std::fprintf(f, "\n");
+  std::fclose(f);
+  if (!m.green_one.empty()) {
+    f = open("cisajs");
+    for (size_t k = 0; k < m.green_one.size(); ++k) {
+      const auto& t = m.green_one[k];
+      std::fprintf(f, "%d %d %d %d %s  %s \n", t.i, t.si, t.j, t.sj, c_double(one[k]).c_str(),
+                   c_double(0.0).c_str());
+    }
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
+  if (!m.green_two_ex.empty()) {
+    f = open("cisajscktaltex");
+    for (size_t k = 0; k < m.green_two_ex.size(); ++k)
+      std::fprintf(f, "%s  %s ", c_double(two_ex[k]).c_str(), c_double(0.0).c_str());
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
+  if (!m.green_two.empty()) {
+    f = open("cisajscktalt");
+    for (size_t k = 0; k < m.green_two.size(); ++k) {
+      const auto& t = m.green_two[k];
+      std::fprintf(f, "%d %d %d %d %d %d %d %d %s %s\n", t.i, t.si, t.j, t.sj, t.k, t.sk, t.l, t.sl,
+                   c_double(two[k]).c_str(), c_double(0.0).c_str());
+    }
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
 }
 
 void write_srinfo_row(const std::string& dir, const Model& m, bool first, const SrInfoRow& r) {

@@ -4,24 +4,31 @@
 // mVMC's Expert-mode definition files that the real normal-orbital optimizer reads
 // (namelist.def, modpara.def, locspn.def, trans.def, coulombintra.def,
 // coulombinter.def, hund.def, gutzwilleridx.def, jastrowidx.def, orbitalidx.def,
-// qptransidx.def), the derived quantum-projection weights, the parameter files
-// (initial.def / zqp_opt.dat triples) and the writers of zvo_out.dat, zvo_var.dat,
-// zvo_SRinfo.dat and zqp_*opt.dat.
+// qptransidx.def) plus the Green-function lists of the PhysCal mode (greenone.def,
+// greentwo.def, greentwoex.def), the derived quantum-projection weights, the parameter
+// files (initial.def / zqp_opt.dat triples) and the writers of zvo_out.dat, zvo_var.dat,
+// zvo_SRinfo.dat, zqp_*opt.dat and the indexed PhysCal files (zvo_out_NNN.dat,
+// zvo_var_NNN.dat, zvo_cisajs_NNN.dat, zvo_cisajscktalt_NNN.dat,
+// zvo_cisajscktaltex_NNN.dat).
 //
 // Reference behaviour followed (paths inside AtelierArith/mvmc-rs):
 //   crates/mvmc-expert-parsers/src/parsers/{modpara,trans,coulomb,gutzwiller,
 //     jastrow,orbital,qptrans,locspin}.rs   file formats (5 header lines, flags)
+//   crates/mvmc-expert-parsers/src/parsers/green.rs:83-270     Green-function lists
+//   crates/mvmc-expert-parsers/src/types.rs:1169-1215          TwoBodyGEx canonical map
 //   crates/mvmc-expert-parsers/src/utils/qp_weight.rs:24-170   QP weights
 //   crates/mvmc-expert-parsers/src/utils/parameter_init.rs:63-260 init + sync
 //   crates/mvmc-core/src/slater_update.rs:17-120               Slater table
 //   crates/mvmc-core/src/qp.rs:33-70                          translated_site
 //   crates/mvmc-core/src/io.rs:142-220,561-730                output files
 //   crates/mvmc-core/src/output_files.rs:55-100               SRinfo rows
+//   crates/mvmc-core/src/io.rs:259-403                        PhysCal output files
 #pragma once
 
 #include <cstdint>
 #include <functional>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace mvmc {
@@ -38,6 +45,16 @@ struct SiteTerm {  // CoulombIntra: U n_i↑ n_i↓
 struct PairTerm {  // CoulombInter: V n_i n_j ; Hund: -J (n_i↑n_j↑ + n_i↓n_j↓)
   int i, j;
   double v;
+};
+
+// Green-function terms of the PhysCal measurement: c†_{i si} c_{j sj} (OneBodyG) and
+// c†_{i si} c_{j sj} c†_{k sk} c_{l sl} (TwoBodyG, the direct "DC" form).
+struct GreenOneTerm {
+  int i, si, j, sj;
+  bool operator==(const GreenOneTerm& o) const { return i == o.i && si == o.si && j == o.j && sj == o.sj; }
+};
+struct GreenTwoTerm {
+  int i, si, j, sj, k, sk, l, sl;
 };
 
 struct Model {
@@ -60,6 +77,13 @@ struct Model {
   std::vector<TransferTerm> transfer;
   std::vector<SiteTerm> coulomb_intra;
   std::vector<PairTerm> coulomb_inter, hund;
+
+  // ---- PhysCal Green-function lists ----
+  // One-body terms: OneBodyG, de-duplicated in order when TwoBodyGEx is present, then the
+  // TwoBodyGEx factors that OneBodyG lacks, appended in TwoBodyGEx order (all are output).
+  std::vector<GreenOneTerm> green_one;
+  std::vector<GreenTwoTerm> green_two;            // TwoBodyG in file order
+  std::vector<std::pair<int, int>> green_two_ex;  // TwoBodyGEx: indices of its two factors
 
   // ---- projection and orbital index tables ----
   int n_gutz = 0, n_jast = 0, n_orb = 0;
@@ -137,5 +161,12 @@ struct OptPoint {
   std::vector<double> params;
 };
 void write_opt_files(const Model& m, const std::string& dir, const std::vector<OptPoint>& window);
+
+// One PhysCal data block (io.rs:259-403): <head>_out_<index>.dat, <head>_var_<index>.dat
+// and, for non-empty lists, <head>_cisajs_, <head>_cisajscktaltex_ and
+// <head>_cisajscktalt_<index>.dat ("%03d" index). `one`, `two_ex` and `two` are the
+// weight-averaged real Green functions in term order; imaginary parts are written as 0.
+void write_physcal_block(const Model& m, const std::string& dir, int index, const StepEnergy& e,
+                         const double* one, const double* two_ex, const double* two);
 
 }  // namespace mvmc

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -805,6 +806,121 @@ double local_energy(const Ctx& c, const int64_t* idx, const int64_t* cfg, const 
   return e + transfer;
 }
 
+// ===================================================================================
+// PhysCal Green functions (observables.rs:558-950,1398,1895-2050; green_measurements.rs:
+// 264-320; run.rs:3352-3420). The PhysCal form of green_func1 / green_func2: projection
+// counts rebuilt by update_proj_cnt, the ratio exp(Σ α Δc) through libm exp, and the
+// Julia complex quotient (pfapack julia_complex.rs:9-75), which for a real numerator a and
+// real denominator c evaluates a·(1/c) (with its power-of-two rescaling at the extremes).
+// ===================================================================================
+double julia_real_quotient(double a, double c) {
+  const double halfov = 0.5 * std::numeric_limits<double>::max();
+  const double twouneps = std::numeric_limits<double>::min() * 2.0 / std::numeric_limits<double>::epsilon();
+  const double ab = std::fabs(a), cd = std::fabs(c);
+  if (std::isinf(c)) return 0.0 * (a == 0.0 ? a : std::copysign(1.0, a)) * std::copysign(1.0, c);
+  double s = 1.0;
+  if (ab >= halfov || ab <= twouneps || cd >= halfov || cd <= twouneps) {
+    const double bs = 2.0 / (std::numeric_limits<double>::epsilon() * std::numeric_limits<double>::epsilon());
+    if (ab >= halfov) {
+      a *= 0.5;
+      s *= 2.0;
+    } else if (ab <= twouneps) {
+      a *= bs;
+      s /= bs;
+    }
+    if (cd >= halfov) {
+      c *= 0.5;
+      s *= 0.5;
+    } else if (cd <= twouneps) {
+      c *= bs;
+      s *= bs;
+    }
+  }
+  const double r = 0.0 / c;
+  const double t = 1.0 / (c + 0.0 * r);
+  return (a + 0.0 * (0.0 / c)) * t * s;
+}
+
+struct GreenSample {
+  const int64_t *idx, *cfg, *num, *cnt;
+  const double *inv, *pf;
+  double ip;
+};
+
+// <c†_{ri,s} c_{rj,t}> of one sample (green_func1_impl, observables.rs:1895-2050).
+double green_one(const Ctx& c, const GreenSample& g, int ri, int rj, int s, int t) {
+  const int ns = c.ns, ne = c.ne, n = c.n;
+  if (g.ip == 0.0) return 0.0;
+  const int dst = ri + s * ns, src = rj + t * ns;
+  if (s == t && ri == rj) return static_cast<double>(g.num[src]);
+  if (s != t) return 0.0;
+  if (g.num[dst] == 1 || g.num[src] == 0) return 0.0;
+  if (g.cfg[src] < 0) return 0.0;
+  const int mj = static_cast<int>(g.cfg[src]);
+  const int msj = mj + t * ne;
+  std::vector<int64_t> idx(g.idx, g.idx + n), num(g.num, g.num + c.ns2), cnt(c.nproj);
+  idx[msj] = ri;
+  num[dst] = 1;
+  num[src] = 0;
+  update_proj_cnt(c, rj, ri, cnt.data(), g.cnt, num.data());
+  const double proj_ratio = c.nproj > 0 ? std::exp(log_proj_ratio(c, cnt.data(), g.cnt)) : 1.0;
+  std::vector<double> pf_new(c.nqp);
+  ratio_hop(c, msj, idx.data(), g.inv, g.pf, pf_new.data());
+  const double new_ip = ip_of(c, pf_new.data());
+  return julia_real_quotient(proj_ratio * new_ip, g.ip);
+}
+
+// <c†_{ri,s} c_{rj,s} c†_{rk,u} c_{rl,u}> of one sample (green_func2_impl,
+// observables.rs:664-860): index coincidences reduce to one-body values or occupations;
+// the general case applies the hop rl→rk (spin u) before rj→ri (spin s).
+double green_two(const Ctx& c, const GreenSample& g, int ri, int rj, int rk, int rl, int s, int u) {
+  const int ns = c.ns, ne = c.ne, n = c.n;
+  if (ne == 0 || ns == 0) return 0.0;
+  auto one = [&](int a, int b, int sp) { return green_one(c, g, a, b, sp, sp); };
+  const int rsi = ri + s * ns, rsj = rj + s * ns, rtk = rk + u * ns;
+  if (s == u) {
+    if (rk == rl) return g.num[rtk] == 0 ? 0.0 : one(ri, rj, s);
+    if (rj == rl) return 0.0;
+    if (ri == rl) {
+      if (g.num[rsi] == 0) return 0.0;
+      if (rj == rk) return static_cast<double>(1 - g.num[rsj]);
+      return -one(rk, rj, s);
+    }
+    if (rj == rk) return g.num[rsj] == 1 ? 0.0 : one(ri, rl, s);
+    if (ri == rk) return 0.0;
+    if (ri == rj) return g.num[rsi] == 0 ? 0.0 : one(rk, rl, s);
+  } else if (rk == rl) {
+    if (g.num[rtk] == 0) return 0.0;
+    if (ri == rj) return static_cast<double>(g.num[rsi]);
+    return one(ri, rj, s);
+  } else if (ri == rj) {
+    return g.num[rsi] == 0 ? 0.0 : one(rk, rl, u);
+  }
+  if (g.num[ri + s * ns] != 0 || g.num[rj + s * ns] != 1 || g.num[rk + u * ns] != 0 || g.num[rl + u * ns] != 1)
+    return 0.0;
+  const int64_t mj = g.cfg[rj + s * ns], mi = g.cfg[rl + u * ns];
+  if (mj < 0 || mi < 0) return 0.0;
+  const int msj = static_cast<int>(mj) + s * ne, msi = static_cast<int>(mi) + u * ne;
+  std::vector<int64_t> idx(g.idx, g.idx + n), num(g.num, g.num + c.ns2), mid(c.nproj), fin(c.nproj);
+  idx[msi] = rk;
+  num[rl + u * ns] = 0;
+  num[rk + u * ns] = 1;
+  update_proj_cnt(c, rl, rk, mid.data(), g.cnt, num.data());
+  idx[msj] = ri;
+  num[rj + s * ns] = 0;
+  num[ri + s * ns] = 1;
+  update_proj_cnt(c, rj, ri, fin.data(), mid.data(), num.data());
+  const double proj_ratio = std::exp(log_proj_ratio(c, fin.data(), g.cnt));
+  std::vector<double> pf_new(c.nqp);
+  // calculate_new_pf_m_two2_real_flat(mi, u, mj, s): electron msa = msi, partner msb = msj
+  if (msi == msj)
+    ratio_hop(c, msj, idx.data(), g.inv, g.pf, pf_new.data());
+  else
+    ratio_exchange(c, msi, msj, idx.data(), g.inv, g.pf, pf_new.data());
+  const double new_ip = ip_of(c, pf_new.data());
+  return julia_real_quotient(proj_ratio * new_ip, g.ip);
+}
+
 // O vector (real slots): [1, proj counts, Slater derivatives].
 void o_vector(const Ctx& c, const int64_t* idx, const int64_t* cnt, const double* inv,
               const double* pf, double ip, double* o) {
@@ -1433,6 +1549,134 @@ int oracle_physcal_samples(const char* namelist, const char* zqp_opt, long long 
       orc::measure(c, w, a);
       energies[2 * b] = a.etot / a.wc;
       energies[2 * b + 1] = a.etot2 / a.wc;
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
+}
+
+int oracle_green_dims(const char* namelist, int* dims, char* err, int err_len) {
+  try {
+    const mvmc::Model m = mvmc::read_expert(namelist);
+    dims[0] = static_cast<int>(m.green_one.size());
+    dims[1] = static_cast<int>(m.green_two_ex.size());
+    dims[2] = static_cast<int>(m.green_two.size());
+    dims[3] = m.data_qty_smp;
+    dims[4] = m.data_idx_start;
+    return 0;
+  } catch (const std::exception& e) {
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
+}
+
+int oracle_physcal_green(const char* namelist, const char* zqp_opt, long long seed, int walkers,
+                         double* energy, double* one, double* ex, double* two, const char* out_dir,
+                         char* err, int err_len) {
+  try {
+    mvmc::Model m = mvmc::read_expert(namelist);
+    std::string why;
+    if (!mvmc::read_para_triples(m, zqp_opt, &why)) throw std::runtime_error("zqp_opt.dat: " + why);
+    mvmc::sync_modified_parameter(m, false);
+    const int W = std::max(1, walkers);
+    std::vector<orc::Walker> ws(W);
+    for (int w = 0; w < W; ++w) {
+      const long long sd = seed + w;
+      if (sd < 0 || sd > 0xffffffffLL) throw std::runtime_error("seed outside the UInt32 range");
+      ws[w].rng.seed(static_cast<uint32_t>(sd));
+      mvmc::Model tmp = m;  // the initial-parameter draws are consumed on a clone
+      mvmc::init_parameter(tmp, [&]() { return ws[w].rng.real2(); });
+    }
+    if (m.nmp_trans < 0) m.nmp_trans = -m.nmp_trans;
+    mvmc::init_qp_weight(m);
+    std::vector<double> slater;
+    mvmc::build_slater_table(m, slater);
+    orc::Ctx c(m, slater);
+    for (auto& w : ws) orc::init_walker(c, w);
+    const int n1 = static_cast<int>(m.green_one.size()), nx = static_cast<int>(m.green_two_ex.size()),
+              n2 = static_cast<int>(m.green_two.size());
+    const int n = c.n, nsamp = m.nvmc_sample;
+    std::vector<double> inv(static_cast<size_t>(c.nqp) * n * n), pf(c.nqp), loc(n1);
+    for (int b = 0; b < m.data_qty_smp; ++b) {
+      double tot[5] = {0, 0, 0, 0, 0};
+      std::vector<double> g1(n1, 0.0), gx(nx, 0.0), g2(n2, 0.0);
+      for (int wi = 0; wi < W; ++wi) {
+        orc::Walker& w = ws[wi];
+        orc::make_sample(c, w);
+        double acc[5] = {0, 0, 0, 0, 0};
+        std::vector<double> s1(n1, 0.0), sx(nx, 0.0), s2(n2, 0.0);
+        for (int s = 0; s < nsamp; ++s) {
+          const int64_t* idx = w.s_idx.data() + static_cast<size_t>(s) * n;
+          bool all_zero = true, all_neg = true;
+          for (int k = 0; k < n; ++k) {
+            all_zero = all_zero && idx[k] == 0;
+            all_neg = all_neg && idx[k] < 0;
+          }
+          if (all_zero || all_neg) continue;
+          if (orc::calc_m_all(c, idx, inv.data(), pf.data()) != 0) continue;
+          const int64_t* cfg = w.s_cfg.data() + static_cast<size_t>(s) * c.ns2;
+          const int64_t* num = w.s_num.data() + static_cast<size_t>(s) * c.ns2;
+          const int64_t* cnt = w.s_cnt.data() + static_cast<size_t>(s) * c.nproj;
+          const double ip = orc::ip_of(c, pf.data());
+          if (std::fabs(ip) < 1.0e-100) continue;
+          const double e = orc::local_energy(c, idx, cfg, num, inv.data(), pf.data(), ip);
+          if (!std::isfinite(e)) continue;
+          double sz = 0.0;
+          for (int r = 0; r < c.ns; ++r) sz += static_cast<double>(num[r] - num[r + c.ns]);
+          acc[0] += 1.0;
+          acc[1] += 1.0 * e;
+          acc[2] += (1.0 * e) * e;
+          acc[3] += 1.0 * sz;
+          acc[4] += 1.0 * sz * sz;
+          const orc::GreenSample gs{idx, cfg, num, cnt, inv.data(), pf.data(), ip};
+          for (int k = 0; k < n1; ++k) {
+            const auto& t = m.green_one[k];
+            loc[k] = orc::green_one(c, gs, t.i, t.j, t.si, t.sj);
+            s1[k] += loc[k];
+          }
+          for (int k = 0; k < nx; ++k) sx[k] += (1.0 * loc[m.green_two_ex[k].first]) * loc[m.green_two_ex[k].second];
+          for (int k = 0; k < n2; ++k) {
+            const auto& t = m.green_two[k];
+            s2[k] += orc::green_two(c, gs, t.i, t.j, t.k, t.l, t.si, t.sk);
+          }
+        }
+        // per-chain normalisation by its own weight, then the chain-order sum
+        const double inv_w = acc[0] != 0.0 ? 1.0 / acc[0] : 1.0;
+        for (int k = 0; k < n1; ++k) g1[k] += s1[k] * inv_w;
+        for (int k = 0; k < nx; ++k) gx[k] += sx[k] * inv_w;
+        for (int k = 0; k < n2; ++k) g2[k] += s2[k] * inv_w;
+        for (int k = 0; k < 5; ++k) tot[k] += acc[k];
+      }
+      if (W > 1) {
+        const double inv_r = 1.0 / W;
+        for (auto& v : g1) v *= inv_r;
+        for (auto& v : gx) v *= inv_r;
+        for (auto& v : g2) v *= inv_r;
+      }
+      mvmc::StepEnergy se;
+      if (std::fabs(tot[0]) >= 1.0e-15) {
+        const double iw = 1.0 / tot[0];
+        se.etot = tot[1] * iw;
+        se.etot2 = tot[2] * iw;
+        se.sztot = tot[3] * iw;
+        se.sztot2 = tot[4] * iw;
+      } else {
+        se.etot = tot[1];
+        se.etot2 = tot[2];
+        se.sztot = tot[3];
+        se.sztot2 = tot[4];
+      }
+      energy[4 * b] = se.etot;
+      energy[4 * b + 1] = se.etot2;
+      energy[4 * b + 2] = se.sztot;
+      energy[4 * b + 3] = se.sztot2;
+      std::copy(g1.begin(), g1.end(), one + static_cast<size_t>(b) * n1);
+      std::copy(gx.begin(), gx.end(), ex + static_cast<size_t>(b) * nx);
+      std::copy(g2.begin(), g2.end(), two + static_cast<size_t>(b) * n2);
+      if (out_dir && *out_dir)
+        mvmc::write_physcal_block(m, out_dir, m.data_idx_start + b, se, g1.data(), gx.data(), g2.data());
     }
     return 0;
   } catch (const std::exception& e) {

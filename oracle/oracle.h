@@ -8,6 +8,8 @@
 //   * SFMT19937 first words per seed (crates/sfmt19937/tests/golden_vs_c.rs)
 //   * every saved configuration, counter, draw count and the next 624 SFMT words of a
 //     native C sampler run (tests/fixtures/native_c_physcal_181/hubbard_chain_real)
+//   * the PhysCal Green functions zvo_cisajs / zvo_cisajscktalt / zvo_cisajscktaltex of
+//     that run on 1, 2 and 4 chains (native_c_physcal_181/hubbard_chain_real{,_mpi2,_mpi4})
 //   * step-1 SR operands E, HO, <O>, <O^2>, last O (tests/fixtures/c_order_sr_operands)
 //   * pfapack identities on tests/fixtures/pfapack/real_n*.orig.txt
 #pragma once
@@ -49,6 +51,21 @@ int oracle_physcal_samples(const char* namelist, const char* zqp_opt, long long 
                            int64_t* ele_idx, int64_t* ele_cfg, int64_t* ele_num,
                            int64_t* proj_cnt, int64_t* counters, int64_t* draws,
                            uint32_t* next624, double* energies, char* err, int err_len);
+
+// Green-function list sizes of a namelist: dims[0] one-body terms (canonical, as output),
+// dims[1] TwoBodyGEx terms, dims[2] TwoBodyG terms, dims[3] NDataQtySmp, dims[4] NDataIdxStart.
+int oracle_green_dims(const char* namelist, int* dims, char* err, int err_len);
+
+// PhysCal run (vmc_phys_cal_in_place_with_options_timed, run.rs:980-1156) with fixed
+// parameters from zqp_opt.dat over `walkers` chains seeded seed + w, each consuming its
+// initial-parameter draws first. For every data block b: energy[4b..] = weight-averaged
+// Etot, Etot2, Sztot, Sztot2; one[b*dims[0]..], ex[b*dims[1]..], two[b*dims[2]..] = the
+// Green functions, each chain's sums scaled by its 1/Wc, summed over chains in order and
+// scaled by 1/walkers (normalize_physcal_green run.rs:287, average_physcal_rank_
+// contributions run.rs:1158). With out_dir non-empty it also writes the block files.
+int oracle_physcal_green(const char* namelist, const char* zqp_opt, long long seed, int walkers,
+                         double* energy, double* one, double* ex, double* two, const char* out_dir,
+                         char* err, int err_len);
 
 // Step 1 of an optimisation with W chains (seed + w): every walker's saved samples,
 // counters, draw counts, the O store [W][S][sr_size] and the reduced operands

@@ -50,8 +50,18 @@ def main(ref):
     copy_tree(os.path.join(src, "inputs"), os.path.join(dst, "inputs"))
     shutil.copyfile(os.path.join(src, "zqp_opt.dat"), os.path.join(dst, "zqp_opt.dat"))
     copy_tree(os.path.join(src, "native-state"), os.path.join(dst, "native-state"))
-    copy_tree(os.path.join(src, "expected"), os.path.join(dst, "expected"),
-              names={"zvo_out_007.dat", "zvo_out_008.dat"})
+    physcal = {f"zvo_{kind}_{idx:03d}.dat" for idx in (7, 8)
+               for kind in ("out", "var", "cisajs", "cisajscktalt", "cisajscktaltex")}
+    copy_tree(os.path.join(src, "expected"), os.path.join(dst, "expected"), names=physcal)
+    # The same inputs run as 2 and 4 MPI ranks (chains seeded RndSeed + rank): only the
+    # C outputs differ.
+    for ranks in (2, 4):
+        other = src + f"_mpi{ranks}"
+        for name in sorted(os.listdir(os.path.join(src, "inputs"))):
+            a = open(os.path.join(src, "inputs", name), "rb").read()
+            b = open(os.path.join(other, "inputs", name), "rb").read()
+            assert a == b, (other, name)
+        copy_tree(os.path.join(other, "expected"), os.path.join(dst, f"expected_mpi{ranks}"), names=physcal)
 
     # Native C step-1 SR operands (energy, HO, <O>, <O^2>, last O) for the Hubbard chain.
     src = os.path.join(fx, "c_order_sr_operands")

@@ -70,6 +70,41 @@ def physcal_samples(namelist, zqp, seed):
     return d, out
 
 
+def green_dims(namelist):
+    dims = (ctypes.c_int * 5)()
+    err = err_buf()
+    if lib().oracle_green_dims(namelist.encode(), dims, err, 1024) != 0:
+        raise RuntimeError(err.value.decode())
+    return dict(zip(["one", "ex", "two", "blocks", "idx_start"], list(dims)))
+
+
+def physcal_green(namelist, zqp, seed, walkers=1, out_dir=""):
+    """PhysCal blocks on `walkers` chains: energies [blocks][4] (Etot, Etot2, Sztot,
+    Sztot2) and the one-body, TwoBodyGEx and TwoBodyG Green functions per block."""
+    g = green_dims(namelist)
+    b = g["blocks"]
+    out = dict(energy=np.zeros((b, 4)), one=np.zeros((b, g["one"])), ex=np.zeros((b, g["ex"])),
+               two=np.zeros((b, g["two"])))
+    err = err_buf()
+    rc = lib().oracle_physcal_green(namelist.encode(), zqp.encode(), ctypes.c_longlong(seed), walkers,
+                                    *(ptr(out[k]) for k in ("energy", "one", "ex", "two")),
+                                    out_dir.encode(), err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return g, out
+
+
+def read_physcal_expected(directory, index):
+    """Numbers of the native C PhysCal files of one data block."""
+    def nums(name, skip):
+        path = os.path.join(directory, f"zvo_{name}_{index:03d}.dat")
+        rows = [line.split() for line in open(path) if line.strip()]
+        return np.array([[float(v) for v in r[skip:]] for r in rows])
+    out = nums("out", 0)[0]
+    return dict(energy=np.array([out[0], out[2], out[4], out[5]]), one=nums("cisajs", 4)[:, 0],
+                two=nums("cisajscktalt", 8)[:, 0], ex=nums("cisajscktaltex", 0)[0, 0::2])
+
+
 def step1_operands(namelist, cg=1, store=0, seed=1):
     d = model_dims(namelist)
     size = 1 + d["npara"]

@@ -166,6 +166,30 @@ int mvmc_b200_status(mvmc_b200_ctx* ctx, unsigned* device_status);
 int mvmc_b200_run_opt(const char* namelist, const char* initial_def, const char* out_dir,
                       const mvmc_b200_options* opt, int nsteps);
 
+/* PhysCal (NVMCCalMode 1) with fixed parameters: replaces prepare_phys_cal_from_namelist
+ * (crates/mvmc-core/src/run.rs:555) and vmc_phys_cal_to_dir (run.rs:751-780). Each walker
+ * consumes its initial-parameter draws (seed + w), then the parameters are read from
+ * zqp_opt (the last 6 + 3·NPara numbers) without the G/J shift and |NMPTrans| is used.
+ * The OneBodyG / TwoBodyG / TwoBodyGEx lists of the namelist are measured. */
+int mvmc_b200_physcal_create(const char* namelist, const char* zqp_opt, const mvmc_b200_options* opt,
+                             mvmc_b200_ctx** out);
+/* dims[5]: one-body terms (OneBodyG after the TwoBodyGEx canonical map, as written to
+ * zvo_cisajs), TwoBodyGEx terms, TwoBodyG terms, NDataQtySmp, NDataIdxStart. */
+int mvmc_b200_green_dims(const mvmc_b200_ctx* ctx, int* dims);
+/* Measurement of the saved samples in the PhysCal form (accumulate_observables with
+ * NVMCCalMode 1, run.rs:3300-3420; ordinary_green_values, observables/
+ * green_measurements.rs:264): energy[5] = Wc, <E>, <E^2>, <Sz>, <Sz^2> (weight-averaged
+ * over all walkers) and the Green functions one[dims[0]], two_ex[dims[1]], two[dims[2]]
+ * (each walker's sums scaled by its 1/Wc, summed over walkers and scaled by 1/W, as
+ * normalize_physcal_green run.rs:287 and average_physcal_rank_contributions run.rs:1158).
+ * No O rows are written. Any output pointer may be null. */
+int mvmc_b200_measure_green(mvmc_b200_ctx* ctx, double* energy, double* one, double* two_ex, double* two);
+/* The PhysCal run: NDataQtySmp blocks of sample → measure, writing zvo_out_NNN.dat,
+ * zvo_var_NNN.dat, zvo_cisajs_NNN.dat, zvo_cisajscktaltex_NNN.dat and
+ * zvo_cisajscktalt_NNN.dat (NNN = NDataIdxStart + block, io.rs:259-403) into out_dir. */
+int mvmc_b200_run_physcal(const char* namelist, const char* zqp_opt, const char* out_dir,
+                          const mvmc_b200_options* opt);
+
 /* Sampler phase timers (the device analogue of the C timers of the sampler substeps):
  * cycles[8] = {candidate, ratio, metropolis, update, refresh, total, -, -} summed over walkers
  * for the last mvmc_b200_sample, measured by each walker's control thread. Zero unless the

@@ -23,7 +23,9 @@ int launch_sample(const DevModel& m, const DevWalkers& w, int precision, cudaStr
 bool sample_planes_in_smem(const DevModel& m, int precision, int limit);
 int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                   double* eloc, double* lpsi, int* valid, unsigned* status, cudaStream_t stream);
+                   double* eloc, double* lpsi, int* valid, double* gval, unsigned* status, cudaStream_t stream);
+int launch_green_reduce(const DevModel& m, int W, int S, int n_one, int nex, const int* ex, const double* gval,
+                        const int* valid, double* out, cudaStream_t stream);
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,
                   const int* valid, const int* s_num, double* wsum, double* tot, cudaStream_t stream);
 int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
@@ -137,6 +139,12 @@ struct mvmc_b200_ctx {
   size_t shard_vec_cap = 0;
   double* d_shard_part = nullptr;
   size_t shard_part_cap = 0;
+  // PhysCal Green functions: per-sample rows, the TwoBodyGEx factor pairs and the result
+  double* d_gval = nullptr;
+  size_t gval_cap = 0;
+  int* d_gex = nullptr;
+  double* d_gout = nullptr;
+  int n_one = 0, n_ex = 0;
   std::vector<double> tot;  // host copy of the last reduction
   long long h2d = 0, d2h = 0;  // bytes copied across the host boundary
   bool sampled = false, measured = false;
@@ -204,7 +212,68 @@ void upload_parameters(mvmc_b200_ctx* c) {
   check(cudaStreamSynchronize(c->stream), "parameter upload");
 }
 
-void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_def, const mvmc_b200_options& opt) {
+// Green tables of the PhysCal measurement. The one-body list is the output list followed
+// by the one-body values that TwoBodyG terms with coincident indices reduce to (the one(...)
+// calls of green_func2_impl, observables.rs:700-745); TwoBodyG terms without a coincidence
+// get a two-hop slot.
+void build_green_tables(mvmc_b200_ctx* c) {
+  const mvmc::Model& m = c->m;
+  std::vector<mvmc::GreenOneTerm> one = m.green_one;
+  auto ref_of = [&](int a, int b, int sp) {
+    const mvmc::GreenOneTerm t{a, sp, b, sp};
+    auto it = std::find(one.begin(), one.end(), t);
+    if (it != one.end()) return static_cast<int>(it - one.begin());
+    one.push_back(t);
+    return static_cast<int>(one.size()) - 1;
+  };
+  std::vector<int> gtwo, ggen;
+  for (const auto& t : m.green_two) {
+    const int ri = t.i, rj = t.j, rk = t.k, rl = t.l, s = t.si, u = t.sk;
+    int ref = -1, gen = -1;
+    bool general = false;
+    if (s == u) {
+      if (rk == rl) ref = ref_of(ri, rj, s);
+      else if (rj == rl) {}
+      else if (ri == rl) { if (rj != rk) ref = ref_of(rk, rj, s); }
+      else if (rj == rk) ref = ref_of(ri, rl, s);
+      else if (ri == rk) {}
+      else if (ri == rj) ref = ref_of(rk, rl, s);
+      else general = true;
+    } else if (rk == rl) {
+      if (ri != rj) ref = ref_of(ri, rj, s);
+    } else if (ri == rj) {
+      ref = ref_of(rk, rl, u);
+    } else {
+      general = true;
+    }
+    if (general) {
+      gen = static_cast<int>(ggen.size() / 6);
+      ggen.insert(ggen.end(), {ri, rj, rk, rl, s, u});
+    }
+    gtwo.insert(gtwo.end(), {ri, rj, rk, rl, s, u, ref, gen});
+  }
+  std::vector<int> gone, gex;
+  for (const auto& t : one) gone.insert(gone.end(), {t.i, t.si, t.j, t.sj});
+  for (const auto& p : m.green_two_ex) gex.insert(gex.end(), {p.first, p.second});
+  DevModel& dm = c->dm;
+  dm.ngone = static_cast<int>(one.size());
+  dm.ngtwo = static_cast<int>(m.green_two.size());
+  dm.nggen = static_cast<int>(ggen.size() / 6);
+  dm.gw = dm.ngone + dm.ngtwo + dm.nggen;
+  dm.gone = c->upload(gone);
+  dm.gtwo = c->upload(gtwo);
+  dm.ggen = c->upload(ggen);
+  c->d_gex = c->upload(gex);
+  c->n_one = static_cast<int>(m.green_one.size());
+  c->n_ex = static_cast<int>(m.green_two_ex.size());
+  c->d_gout = c->alloc<double>(c->n_one + c->n_ex + dm.ngtwo);
+}
+
+// physcal_zqp (PhysCal, prepare_phys_cal_from_namelist run.rs:555-737): every walker still
+// consumes its initial-parameter draws, then the fixed parameters are read from zqp_opt.dat
+// and synchronised without the Gutzwiller/Jastrow shift, and NMPTrans is taken by magnitude.
+void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_def, const mvmc_b200_options& opt,
+                   const char* physcal_zqp = nullptr) {
   c->opt = opt;
   check(cudaSetDevice(opt.device), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -236,11 +305,19 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
       m.slater = tmp.slater;
     }
   }
-  if (initial_def && *initial_def) {
+  if (physcal_zqp) {
     std::string why;
-    if (!mvmc::read_para_triples(m, initial_def, &why)) throw std::runtime_error(std::string("initial.def: ") + why);
+    if (!mvmc::read_para_triples(m, physcal_zqp, &why)) throw std::runtime_error(std::string("zqp_opt.dat: ") + why);
+    mvmc::sync_modified_parameter(m, false);
+    if (m.nmp_trans < 0) m.nmp_trans = -m.nmp_trans;
+    m.calc_mode = 1;
+  } else {
+    if (initial_def && *initial_def) {
+      std::string why;
+      if (!mvmc::read_para_triples(m, initial_def, &why)) throw std::runtime_error(std::string("initial.def: ") + why);
+    }
+    mvmc::sync_modified_parameter(m, true);
   }
-  mvmc::sync_modified_parameter(m, true);
   mvmc::init_qp_weight(m);
 
   const int ns = m.nsite, n = m.nsize(), ns2 = 2 * ns, nqp = m.nqp, nproj = m.nproj();
@@ -362,6 +439,7 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   c->d_gws = c->alloc<double>(static_cast<size_t>(c->gws_blocks) * 2 * nn);
   c->d_red = c->alloc<double>(4096);
   c->d_scal = c->alloc<double>(8);
+  build_green_tables(c);
   upload_parameters(c);
 }
 
@@ -383,7 +461,8 @@ int guarded(F&& f) {
 int do_measure(mvmc_b200_ctx* c) {
   const int rows = c->W * c->S;
   int rc = launch_measure(c->dm, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, rows, c->d_gws,
-                          c->gws_blocks, c->d_ostore, c->d_eloc, c->d_lpsi, c->d_valid, c->dw.status, c->stream);
+                          c->gws_blocks, c->d_ostore, c->d_eloc, c->d_lpsi, c->d_valid, nullptr, c->dw.status,
+                          c->stream);
   if (rc != kOk) return rc;
   rc = launch_reduce(c->dm, c->W, c->S, c->d_ostore, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
                      c->stream);
@@ -394,6 +473,45 @@ int do_measure(mvmc_b200_ctx* c) {
   c->d2h += static_cast<long long>(sizeof(double) * c->tot.size());
   check(cudaStreamSynchronize(c->stream), "measure");
   c->measured = true;
+  return kOk;
+}
+
+// PhysCal measurement of the saved samples (accumulate_observables with NVMCCalMode 1,
+// run.rs:3300-3420): energies and Green functions, no O rows. tot[0..4] receives
+// Wc, <E>, <E^2>, <Sz>, <Sz^2>; gout the Green functions (one-body, TwoBodyGEx, TwoBodyG).
+int do_measure_green(mvmc_b200_ctx* c, std::vector<double>& gout) {
+  const size_t rows = static_cast<size_t>(c->W) * c->S;
+  const size_t need = rows * std::max(1, c->dm.gw);
+  if (need > c->gval_cap) {
+    if (c->d_gval) {
+      check(cudaFree(c->d_gval), "cudaFree");
+      c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), static_cast<void*>(c->d_gval)));
+    }
+    c->d_gval = c->alloc<double>(need);
+    c->gval_cap = need;
+  }
+  int rc = launch_measure(c->dm, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, static_cast<int>(rows), c->d_gws,
+                          c->gws_blocks, nullptr, c->d_eloc, c->d_lpsi, c->d_valid, c->d_gval, c->dw.status,
+                          c->stream);
+  if (rc != kOk) return rc;
+  DevModel energy_only = c->dm;
+  energy_only.sr_size = 0;
+  rc = launch_reduce(energy_only, c->W, c->S, nullptr, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
+                     c->stream);
+  if (rc != kOk) return rc;
+  rc = launch_green_reduce(c->dm, c->W, c->S, c->n_one, c->n_ex, c->d_gex, c->d_gval, c->d_valid, c->d_gout,
+                           c->stream);
+  if (rc != kOk) return rc;
+  c->tot.assign(5, 0.0);
+  check(cudaMemcpyAsync(c->tot.data(), c->d_tot, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream),
+        "download reduction");
+  gout.assign(static_cast<size_t>(c->n_one) + c->n_ex + c->dm.ngtwo, 0.0);
+  if (!gout.empty())
+    check(cudaMemcpyAsync(gout.data(), c->d_gout, sizeof(double) * gout.size(), cudaMemcpyDeviceToHost, c->stream),
+          "download Green functions");
+  c->d2h += static_cast<long long>(sizeof(double) * (5 + gout.size()));
+  check(cudaStreamSynchronize(c->stream), "measure Green functions");
+  c->measured = false;  // the O rows were not written
   return kOk;
 }
 
@@ -887,6 +1005,77 @@ extern "C" int mvmc_b200_run_opt(const char* namelist, const char* initial_def, 
       if (step >= window_start) window.push_back({t[1], t[2], mvmc::all_parameters(m)});
     }
     mvmc::write_opt_files(m, out_dir, window);
+    return MVMC_B200_OK;
+  });
+  mvmc_b200_destroy(c);
+  return rc;
+}
+
+// ---------------------------------------------------------------------------------------
+// PhysCal (NVMCCalMode 1): fixed parameters, energies and Green functions per data block
+// (vmc_phys_cal_in_place_with_options_timed, crates/mvmc-core/src/run.rs:980-1156).
+// ---------------------------------------------------------------------------------------
+extern "C" int mvmc_b200_physcal_create(const char* namelist, const char* zqp_opt, const mvmc_b200_options* opt,
+                                        mvmc_b200_ctx** out) {
+  if (!namelist || !zqp_opt || !out) return MVMC_B200_EARG;
+  *out = nullptr;
+  mvmc_b200_options o;
+  mvmc_b200_default_options(&o);
+  if (opt) o = *opt;
+  return guarded([&]() {
+    auto* c = new mvmc_b200_ctx();
+    try {
+      build_context(c, namelist, nullptr, o, zqp_opt);
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_green_dims(const mvmc_b200_ctx* c, int* dims) {
+  if (!c || !dims) return MVMC_B200_EARG;
+  const int v[5] = {c->n_one, c->n_ex, c->dm.ngtwo, c->m.data_qty_smp, c->m.data_idx_start};
+  std::copy(v, v + 5, dims);
+  return MVMC_B200_OK;
+}
+
+extern "C" int mvmc_b200_measure_green(mvmc_b200_ctx* c, double* energy, double* one, double* two_ex, double* two) {
+  if (!c) return MVMC_B200_EARG;
+  if (!c->sampled) return MVMC_B200_ESTATE;
+  return guarded([&]() {
+    std::vector<double> g;
+    const int rc = do_measure_green(c, g);
+    if (rc != kOk) return rc;
+    if (energy) std::copy(c->tot.begin(), c->tot.begin() + 5, energy);
+    if (one) std::copy(g.begin(), g.begin() + c->n_one, one);
+    if (two_ex) std::copy(g.begin() + c->n_one, g.begin() + c->n_one + c->n_ex, two_ex);
+    if (two) std::copy(g.begin() + c->n_one + c->n_ex, g.end(), two);
+    return MVMC_B200_OK;
+  });
+}
+
+extern "C" int mvmc_b200_run_physcal(const char* namelist, const char* zqp_opt, const char* out_dir,
+                                     const mvmc_b200_options* opt) {
+  if (!namelist || !zqp_opt || !out_dir) return MVMC_B200_EARG;
+  mvmc_b200_ctx* c = nullptr;
+  int rc = mvmc_b200_physcal_create(namelist, zqp_opt, opt, &c);
+  if (rc != MVMC_B200_OK) return rc;
+  rc = guarded([&]() {
+    const mvmc::Model& m = c->m;
+    for (int b = 0; b < std::max(0, m.data_qty_smp); ++b) {
+      int r = launch_sample(c->dm, c->dw, c->opt.precision, c->stream);
+      if (r != kOk) return r;
+      c->sampled = true;
+      std::vector<double> g;
+      r = do_measure_green(c, g);
+      if (r != kOk) return r;
+      const double* t = c->tot.data();
+      mvmc::write_physcal_block(m, out_dir, m.data_idx_start + b, mvmc::StepEnergy{t[1], t[2], t[3], t[4]}, g.data(),
+                                g.data() + c->n_one, g.data() + c->n_one + c->n_ex);
+    }
     return MVMC_B200_OK;
   });
   mvmc_b200_destroy(c);

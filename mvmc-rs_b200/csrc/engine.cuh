@@ -36,6 +36,14 @@ struct DevModel {
   const double* inter_v;
   const int* hund_ij;      // [nhund*2]
   const double* hund_v;
+  // PhysCal Green functions. One-body terms: the output list first, then the one-body
+  // values that coincident-index TwoBodyG terms reduce to. TwoBodyG terms carry the index
+  // of that one-body value (ref, or -1) and of their two-hop slot (gen, or -1). A measured
+  // sample's row holds [ngone one-body | ngtwo two-body | nggen two-hop] values (width gw).
+  int ngone = 0, ngtwo = 0, nggen = 0, gw = 0;
+  const int* gone = nullptr;  // [ngone*4]: i, s, j, t of c†_{i s} c_{j t}
+  const int* gtwo = nullptr;  // [ngtwo*8]: ri, rj, rk, rl, s, u, ref, gen
+  const int* ggen = nullptr;  // [nggen*6]: ri, rj, rk, rl, s, u of the two-hop terms
 };
 
 // Per-walker persistent state, arrays of W entries each.

@@ -10,12 +10,19 @@
 //   * O = [1, projection counts, ∂lnΨ/∂f_k] (set_projection_diff observables.rs:202 and the
 //     adjoint Slater derivative slater_derivative.rs:289-550), written as one row of the
 //     SR sample matrix (calculate_oo_store_real, observables.rs:297).
+// In the PhysCal form (NVMCCalMode 1) the O row is skipped and the Green functions of
+// the sample are evaluated on the same inverse planes instead (ordinary_green_values,
+// crates/mvmc-core/src/observables/green_measurements.rs:264-320): one-body terms by the
+// one-electron ratio (green_func1, observables.rs:1895-2050), TwoBodyG terms by their
+// index-coincidence reductions or the two-hop ratio (green_func2, observables.rs:664-860;
+// two_ratio_real, sampling/updates.rs:1539-1567).
 // The reductions sum per walker in sample order and then across walkers in walker
 // order (the rank-order fold of ThreadReducer, multichain.rs:433), so reruns are
 // bitwise repeatable up to the O_k scatter (shared-memory atomics).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -26,12 +33,12 @@ namespace mvmcb {
 constexpr int kMeasThreads = 256;
 
 struct MeasLayout {
-  size_t idx, cfg, num, cnt, tr, sg, pf, tacc, g1, oacc, cj, gj, plane, total;
+  size_t idx, cfg, num, cnt, tr, sg, pf, tacc, g1, oacc, cj, gscr, gj, plane, total;
 };
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_plane) {
+__host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_plane, bool green = false) {
   MeasLayout L;
   size_t o = 0;
   L.idx = o; o = a16(o + sizeof(int) * m.n);
@@ -45,6 +52,9 @@ __host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_p
   L.g1 = o; o = a16(o + sizeof(double) * (m.nterm + 1));
   L.oacc = o; o = a16(o + sizeof(double) * (m.norb + 1));
   L.cj = o; o = a16(o + sizeof(double) * m.ns);
+  // two-hop scratch: the gathered Slater rows u, v of one term per warp
+  L.gscr = o;
+  if (green && m.nggen > 0) o = a16(o + sizeof(double) * 2 * (kMeasThreads / 32) * static_cast<size_t>(m.n));
   L.gj = o;
   L.plane = o;
   // the plane and its ping-pong partner
@@ -53,14 +63,179 @@ __host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_p
   return L;
 }
 
-template <int JPL, bool kSmemPlane>
+// Σ_k α_k Δc_k of moving one electron from site `src` to site `dst` (update_proj_cnt,
+// sampling/projection.rs:278, with log_proj_ratio :403), where occ(slot) is the occupation
+// of the 2Ns spin-site slots after the move: Gutzwiller −α(src)·n_src + α(dst)·n↑n↓(dst),
+// Jastrow α(src,dst)·(n_src − n_dst + 1) + Σ_{k≠src,dst} (α(dst,k) − α(src,k))·(n_k − 1).
+template <class Occ>
+__device__ double hop_log_proj(const DevModel& m, int src, int dst, Occ occ) {
+  const int ns = m.ns;
+  const int n_src = occ(src) + occ(src + ns), n_dst = occ(dst) + occ(dst + ns);
+  double z = -m.gutz_site[src] * static_cast<double>(n_src);
+  z += m.gutz_site[dst] * static_cast<double>(occ(dst) * occ(dst + ns));
+  z += m.jast_pair[src * ns + dst] * static_cast<double>(n_src - n_dst + 1);
+  for (int k = 0; k < ns; ++k) {
+    if (k == src || k == dst) continue;
+    z += (m.jast_pair[dst * ns + k] - m.jast_pair[src * ns + k]) * static_cast<double>(occ(k) + occ(k + ns) - 1);
+  }
+  return z;
+}
+
+// Julia's complex quotient (pfapack julia_complex.rs:9-75) for a real numerator a and a
+// real denominator c: a·(1/c), rescaled by powers of two when |a| or |c| is extreme.
+__device__ inline double julia_real_quotient(double a, double c) {
+  const double halfov = 0.5 * DBL_MAX, twouneps = DBL_MIN * 2.0 / DBL_EPSILON;
+  const double ab = fabs(a), cd = fabs(c);
+  if (isinf(c)) return 0.0 * (a == 0.0 ? a : copysign(1.0, a)) * copysign(1.0, c);
+  double s = 1.0;
+  if (ab >= halfov || ab <= twouneps || cd >= halfov || cd <= twouneps) {
+    const double bs = 2.0 / (DBL_EPSILON * DBL_EPSILON);
+    if (ab >= halfov) { a *= 0.5; s *= 2.0; }
+    else if (ab <= twouneps) { a *= bs; s /= bs; }
+    if (cd >= halfov) { c *= 0.5; s *= 0.5; }
+    else if (cd <= twouneps) { c *= bs; s *= bs; }
+  }
+  const double t = 1.0 / c;
+  return a * t * s;
+}
+
+// Per-plane Green contributions of one sample: Σ_q w_q·Pf'_q of every one-body hop and of
+// every two-hop term, added into the sample's row (plane order).
+template <int JPL>
+__device__ void green_plane(const DevModel& m, int q, double wq, double pfv, const double* A, const int* idx,
+                            const int* cfg, const int* num, double* grow, double* gscr) {
+  const int n = m.n, ns = m.ns, ne = m.ne, lane = threadIdx.x & 31, warp = threadIdx.x >> 5,
+            nwarp = blockDim.x >> 5;
+  // one-body: the electron at rj (spin t) moves to the empty ri: Pf' = −Pf·Σ_k X⁻¹[msj][k]·F(ri, r'_k)
+  for (int k = warp; k < m.ngone; k += nwarp) {
+    const int gi = m.gone[4 * k], gs = m.gone[4 * k + 1], gj = m.gone[4 * k + 2], gt = m.gone[4 * k + 3];
+    const int dst = gi + gs * ns, src = gj + gt * ns;
+    if (gs != gt || gi == gj || num[dst] == 1 || num[src] == 0 || cfg[src] < 0) continue;
+    const int msj = cfg[src] + gt * ne;
+    const double* row = A + static_cast<size_t>(msj) * n;
+    const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + (gi + gt * ns)) * m.ns2;
+    double r = 0.0;
+    for (int c = lane; c < n; c += 32) {
+      const int rc = (c == msj ? gi : idx[c]) + (c >= ne ? ns : 0);
+      r += row[c] * __ldg(srow + rc);
+    }
+    r = warp_sum(r);
+    if (lane == 0) grow[k] += wq * (-r * pfv);
+  }
+  // two-hop: electron msa moves rl → rk (spin u), then msb moves rj → ri (spin s);
+  // ratio = X_ab·v_a + X_ab·(vᵀ X u) + p_a q_b − p_b q_a with u, v the moved rows
+  double* gu = gscr + static_cast<size_t>(warp) * 2 * n;
+  double* gv = gu + n;
+  for (int g = warp; g < m.nggen; g += nwarp) {
+    const int* t = m.ggen + 6 * g;
+    const int ri = t[0], rj = t[1], rk = t[2], rl = t[3], s = t[4], u = t[5];
+    if (num[ri + s * ns] != 0 || num[rj + s * ns] != 1 || num[rk + u * ns] != 0 || num[rl + u * ns] != 1) continue;
+    const int mj = cfg[rj + s * ns], mi = cfg[rl + u * ns];
+    if (mj < 0 || mi < 0) continue;
+    const int msa = mi + u * ne, msb = mj + s * ne;
+    const double* sa = m.slater + (static_cast<size_t>(q) * m.ns2 + (rk + u * ns)) * m.ns2;
+    const double* sb = m.slater + (static_cast<size_t>(q) * m.ns2 + (ri + s * ns)) * m.ns2;
+    const double* xa = A + static_cast<size_t>(msa) * n;
+    const double* xb = A + static_cast<size_t>(msb) * n;
+    double pa = 0.0, pb = 0.0, qa = 0.0, qb = 0.0;
+    for (int c = lane; c < n; c += 32) {
+      const int rc = (c == msa ? rk : (c == msb ? ri : idx[c])) + (c >= ne ? ns : 0);
+      const double va = __ldg(sa + rc), vb = __ldg(sb + rc);
+      gu[c] = va;
+      gv[c] = vb;
+      pa += xa[c] * va;
+      pb += xb[c] * va;
+      qa += xa[c] * vb;
+      qb += xb[c] * vb;
+    }
+    __syncwarp();
+    // vᵀ X u: column sums w_c = Σ_i v_i X[i][c] (lanes on consecutive columns), then Σ_c w_c u_c
+    double bma = 0.0;
+    for (int c = lane; c < n; c += 32) {
+      double w = 0.0;
+      for (int i = 0; i < n; ++i) w += gv[i] * A[static_cast<size_t>(i) * n + c];
+      bma += w * gu[c];
+    }
+    pa = warp_sum(pa);
+    pb = warp_sum(pb);
+    qa = warp_sum(qa);
+    qb = warp_sum(qb);
+    bma = warp_sum(bma);
+    if (lane == 0) {
+      const double xab = xa[msb], vba = gv[msa];
+      const double ratio = xab * vba + xab * bma + pa * qb - pb * qa;
+      grow[m.ngone + m.ngtwo + g] += wq * (ratio * pfv);
+    }
+    __syncwarp();
+  }
+}
+
+// Final Green values of one sample from the plane sums (run after the energy, all threads).
+__device__ void green_finish(const DevModel& m, double ip, bool ok, const int* cfg, const int* num, double* grow) {
+  const int ns = m.ns, tid = threadIdx.x, nt = blockDim.x;
+  for (int k = tid; k < m.ngone; k += nt) {
+    const int gi = m.gone[4 * k], gs = m.gone[4 * k + 1], gj = m.gone[4 * k + 2], gt = m.gone[4 * k + 3];
+    const int dst = gi + gs * ns, src = gj + gt * ns;
+    double v;
+    if (ip == 0.0) v = 0.0;
+    else if (gs == gt && gi == gj) v = static_cast<double>(num[src]);
+    else if (gs != gt || num[dst] == 1 || num[src] == 0 || cfg[src] < 0) v = 0.0;
+    else {
+      auto occ = [&](int slot) { return slot == src ? 0 : (slot == dst ? 1 : num[slot]); };
+      v = julia_real_quotient(exp(hop_log_proj(m, gj, gi, occ)) * grow[k], ip);
+    }
+    grow[k] = ok ? v : 0.0;
+  }
+  for (int g = tid; g < m.nggen; g += nt) {
+    const int* t = m.ggen + 6 * g;
+    const int ri = t[0], rj = t[1], rk = t[2], rl = t[3], s = t[4], u = t[5];
+    double v = 0.0;
+    if (ip != 0.0 && num[ri + s * ns] == 0 && num[rj + s * ns] == 1 && num[rk + u * ns] == 0 &&
+        num[rl + u * ns] == 1 && cfg[rj + s * ns] >= 0 && cfg[rl + u * ns] >= 0) {
+      const int a0 = rl + u * ns, a1 = rk + u * ns, b0 = rj + s * ns, b1 = ri + s * ns;
+      auto mid = [&](int slot) { return slot == a0 ? 0 : (slot == a1 ? 1 : num[slot]); };
+      auto fin = [&](int slot) { return slot == b0 ? 0 : (slot == b1 ? 1 : mid(slot)); };
+      const double z = hop_log_proj(m, rl, rk, mid) + hop_log_proj(m, rj, ri, fin);
+      v = julia_real_quotient(exp(z) * grow[m.ngone + m.ngtwo + g], ip);
+    }
+    grow[m.ngone + m.ngtwo + g] = ok ? v : 0.0;
+  }
+  __syncthreads();
+  const double* one = grow;
+  const double* gen = grow + m.ngone + m.ngtwo;
+  for (int k = tid; k < m.ngtwo; k += nt) {
+    const int* t = m.gtwo + 8 * k;
+    const int ri = t[0], rj = t[1], rk = t[2], rl = t[3], s = t[4], u = t[5], ref = t[6], gi = t[7];
+    const int rsi = ri + s * ns, rsj = rj + s * ns, rtk = rk + u * ns;
+    double v;
+    if (s == u) {
+      if (rk == rl) v = num[rtk] == 0 ? 0.0 : one[ref];
+      else if (rj == rl) v = 0.0;
+      else if (ri == rl) v = num[rsi] == 0 ? 0.0 : (rj == rk ? static_cast<double>(1 - num[rsj]) : -one[ref]);
+      else if (rj == rk) v = num[rsj] == 1 ? 0.0 : one[ref];
+      else if (ri == rk) v = 0.0;
+      else if (ri == rj) v = num[rsi] == 0 ? 0.0 : one[ref];
+      else v = gen[gi];
+    } else if (rk == rl) {
+      v = num[rtk] == 0 ? 0.0 : (ri == rj ? static_cast<double>(num[rsi]) : one[ref]);
+    } else if (ri == rj) {
+      v = num[rsi] == 0 ? 0.0 : one[ref];
+    } else {
+      v = gen[gi];
+    }
+    grow[m.ngone + k] = ok ? v : 0.0;
+  }
+  __syncthreads();
+}
+
+template <int JPL, bool kSmemPlane, bool kGreen>
 __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
     k_measure(DevModel m, const int* __restrict__ s_idx, const int* __restrict__ s_cfg,
               const int* __restrict__ s_num, const int* __restrict__ s_cnt, int nsamples,
               double* __restrict__ gws, double* __restrict__ ostore, double* __restrict__ eloc,
-              double* __restrict__ lpsi, int* __restrict__ valid, unsigned* status) {
+              double* __restrict__ lpsi, int* __restrict__ valid, double* __restrict__ gval, unsigned* status) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const MeasLayout L = meas_layout(m, kSmemPlane);
+  const MeasLayout L = meas_layout(m, kSmemPlane, kGreen);
   int* idx = reinterpret_cast<int*>(smem + L.idx);
   int* cfg = reinterpret_cast<int*>(smem + L.cfg);
   int* num = reinterpret_cast<int*>(smem + L.num);
@@ -72,6 +247,7 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
   double* g1 = reinterpret_cast<double*>(smem + L.g1);
   double* oacc = reinterpret_cast<double*>(smem + L.oacc);
   double* cj = reinterpret_cast<double*>(smem + L.cj);
+  double* gscr = reinterpret_cast<double*>(smem + L.gscr);
   const int n = m.n, ns = m.ns, ne = m.ne, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   const size_t nn = static_cast<size_t>(n) * n;
@@ -88,6 +264,9 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
     for (int k = tid; k < m.nproj; k += nt) cnt[k] = s_cnt[static_cast<size_t>(sample) * m.nproj + k];
     for (int k = tid; k < m.nterm; k += nt) tacc[k] = 0.0;
     for (int k = tid; k < m.norb; k += nt) oacc[k] = 0.0;
+    double* grow = kGreen ? gval + static_cast<size_t>(sample) * m.gw : nullptr;
+    if (kGreen)
+      for (int k = tid; k < m.gw; k += nt) grow[k] = 0.0;
     if (tid == 0) s_bad = 0;
     __syncthreads();
     // direct projection helper: cj[r] = Σ_site J[r][site]·(n_site − 1)
@@ -112,7 +291,8 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
         eloc[sample] = 0.0;
         lpsi[sample] = 0.0;
       }
-      for (int k = tid; k < m.sr_size; k += nt) ostore[static_cast<size_t>(sample) * m.sr_size + k] = 0.0;
+      if (!kGreen)
+        for (int k = tid; k < m.sr_size; k += nt) ostore[static_cast<size_t>(sample) * m.sr_size + k] = 0.0;
       __syncthreads();
       continue;
     }
@@ -151,6 +331,11 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
         r = warp_sum(r);
         if (lane == 0) tacc[t] += wq * (-r * pfv);
       }
+      if (kGreen) {
+        green_plane<JPL>(m, q, wq, pfv, A, idx, cfg, num, grow, gscr);
+        __syncthreads();
+        continue;  // PhysCal: no O row
+      }
       // adjoint Slater derivative: translated sites of the electrons for this plane
       const int trans = q / m.nleg, spidx = q % m.nleg;
       const int mpidx = trans % m.nmp;
@@ -179,7 +364,10 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
         lpsi[sample] = 0.0;
         atomicOr(status, kDevSingular);
       }
-      for (int k = tid; k < m.sr_size; k += nt) ostore[static_cast<size_t>(sample) * m.sr_size + k] = 0.0;
+      if (kGreen)
+        for (int k = tid; k < m.gw; k += nt) grow[k] = 0.0;
+      else
+        for (int k = tid; k < m.sr_size; k += nt) ostore[static_cast<size_t>(sample) * m.sr_size + k] = 0.0;
       __syncthreads();
       continue;
     }
@@ -242,6 +430,10 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
     }
     __syncthreads();
     const bool ok = pf[m.nqp + 1] != 0.0;
+    if (kGreen) {
+      green_finish(m, ip, ok, cfg, num, grow);
+      continue;
+    }
     const double inv_ip = ip / (ip * ip);
     double* orow = ostore + static_cast<size_t>(sample) * m.sr_size;
     for (int k = tid; k < m.sr_size; k += nt) {
@@ -318,20 +510,20 @@ __global__ void k_weight_average(int size, double* tot) {
 
 size_t measure_smem(const DevModel& m, bool smem_plane) { return meas_layout(m, smem_plane).total; }
 
-template <int JPL>
-int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
-                       const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                       double* eloc, double* lpsi, int* valid, unsigned* status, cudaStream_t stream, int limit) {
-  const bool smem_plane = meas_layout(m, true).total <= static_cast<size_t>(limit);
-  const size_t smem = meas_layout(m, smem_plane).total;
+template <int JPL, bool kGreen>
+int launch_measure_kind(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num, const int* s_cnt,
+                        int nsamples, double* gws, int gws_blocks, double* ostore, double* eloc, double* lpsi,
+                        int* valid, double* gval, unsigned* status, cudaStream_t stream, int limit) {
+  const bool smem_plane = meas_layout(m, true, kGreen).total <= static_cast<size_t>(limit);
+  const size_t smem = meas_layout(m, smem_plane, kGreen).total;
   if (smem > static_cast<size_t>(limit)) return kErrArgument;
   if (smem_plane) {
-    auto kernel = k_measure<JPL, true>;
+    auto kernel = k_measure<JPL, true, kGreen>;
     MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     kernel<<<nsamples, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
-                                                     valid, status);
+                                                     valid, gval, status);
   } else {
-    auto kernel = k_measure<JPL, false>;
+    auto kernel = k_measure<JPL, false, kGreen>;
     MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     // As many blocks as are co-resident, striding over the samples: each block reuses its
     // own ping-pong workspace, so the workspaces stay in L2 across samples.
@@ -341,25 +533,83 @@ int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, co
     MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kMeasThreads, smem));
     const int grid = std::max(1, std::min({nsamples, gws_blocks, sms * std::max(1, per)}));
     kernel<<<grid, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
-                                                 valid, status);
+                                                 valid, gval, status);
   }
   MVMCB_CUDA(cudaGetLastError());
   return kOk;
 }
 
+template <int JPL>
+int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num, const int* s_cnt,
+                       int nsamples, double* gws, int gws_blocks, double* ostore, double* eloc, double* lpsi,
+                       int* valid, double* gval, unsigned* status, cudaStream_t stream, int limit) {
+  if (gval)
+    return launch_measure_kind<JPL, true>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc,
+                                          lpsi, valid, gval, status, stream, limit);
+  return launch_measure_kind<JPL, false>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc,
+                                         lpsi, valid, gval, status, stream, limit);
+}
+
+// gval != nullptr selects the PhysCal form: Green rows [nsamples][m.gw] instead of O rows.
 int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
-                   double* eloc, double* lpsi, int* valid, unsigned* status, cudaStream_t stream) {
+                   double* eloc, double* lpsi, int* valid, double* gval, unsigned* status, cudaStream_t stream) {
   int dev = 0, limit = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int n = m.n;
-  if (n <= 32) return launch_measure_jpl<1>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
-  if (n <= 64) return launch_measure_jpl<2>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
-  if (n <= 128) return launch_measure_jpl<4>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
-  if (n <= 224) return launch_measure_jpl<7>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
-  if (n <= 256) return launch_measure_jpl<8>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, status, stream, limit);
+#define MVMCB_MEASURE(J) \
+  launch_measure_jpl<J>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, gval, \
+                        status, stream, limit)
+  if (n <= 32) return MVMCB_MEASURE(1);
+  if (n <= 64) return MVMCB_MEASURE(2);
+  if (n <= 128) return MVMCB_MEASURE(4);
+  if (n <= 224) return MVMCB_MEASURE(7);
+  if (n <= 256) return MVMCB_MEASURE(8);
+#undef MVMCB_MEASURE
   return kErrArgument;
+}
+
+// PhysCal Green functions of the measured samples: out = [one-body (n_one) | TwoBodyGEx
+// (pairs of one-body values, one per ex entry) | TwoBodyG (ngtwo)]. Every walker's sums in
+// sample order over its valid samples are scaled by its 1/Wc, summed in walker order and
+// scaled by 1/W (normalize_physcal_green run.rs:287-316; average_physcal_rank_contributions
+// run.rs:1158-1181; accumulate_two_body_gex_sample observables.rs:110-126).
+__global__ void k_green_reduce(int W, int S, int gw, int n_one, int two_off, int ngtwo, int nex, const int* __restrict__ ex,
+                               const double* __restrict__ gval, const int* __restrict__ valid, double* __restrict__ out) {
+  const int width = n_one + nex + ngtwo;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < width; k += gridDim.x * blockDim.x) {
+    double tot = 0.0;
+    for (int w = 0; w < W; ++w) {
+      double wc = 0.0, acc = 0.0;
+      for (int s = 0; s < S; ++s) {
+        const size_t smp = static_cast<size_t>(w) * S + s;
+        if (!valid[smp]) continue;
+        const double* row = gval + smp * gw;
+        wc += 1.0;
+        double v;
+        if (k < n_one) v = row[k];
+        else if (k < n_one + nex) v = (1.0 * row[ex[2 * (k - n_one)]]) * row[ex[2 * (k - n_one) + 1]];
+        else v = row[two_off + (k - n_one - nex)];
+        acc += v;
+      }
+      if (wc != 0.0) acc *= 1.0 / wc;
+      tot += acc;
+    }
+    if (W > 1) tot *= 1.0 / W;
+    out[k] = tot;
+  }
+}
+
+int launch_green_reduce(const DevModel& m, int W, int S, int n_one, int nex, const int* ex, const double* gval,
+                        const int* valid, double* out, cudaStream_t stream) {
+  const int width = n_one + nex + m.ngtwo;
+  if (width == 0) return kOk;
+  // the TwoBodyG values sit after all ngone one-body values of the row
+  k_green_reduce<<<(width + 127) / 128, 128, 0, stream>>>(W, S, m.gw, n_one, m.ngone, m.ngtwo, nex, ex, gval, valid,
+                                                          out);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
 }
 
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,

@@ -26,7 +26,8 @@ EXPORTS = [
     "mvmc_b200_stage_propose_exchange", "mvmc_b200_stage_accept_exchange", "mvmc_b200_stage_recompute",
     "mvmc_b200_stage_state", "mvmc_b200_gram", "mvmc_b200_cholesky_solve",
     "mvmc_b200_measure_sums", "mvmc_b200_sr_gather", "mvmc_b200_sr_local_product", "mvmc_b200_sr_apply",
-    "mvmc_b200_sr_config",
+    "mvmc_b200_sr_config", "mvmc_b200_physcal_create", "mvmc_b200_green_dims", "mvmc_b200_measure_green",
+    "mvmc_b200_run_physcal",
 ]
 
 
@@ -137,11 +138,20 @@ def default_options(**kw):
 class Engine:
     """Walker-ensemble engine: sample → measure → SR-CG on the device."""
 
-    def __init__(self, namelist, initial_def="", **options):
+    def __init__(self, namelist, initial_def="", physcal_zqp=None, **options):
+        """physcal_zqp: a zqp_opt.dat path selects the PhysCal form (fixed parameters,
+        Green functions); otherwise initial_def optionally seeds the optimisation."""
         self.opt = default_options(**options)
         self.ctx = ctypes.c_void_p()
-        _check(lib().mvmc_b200_create(namelist.encode(), (initial_def or "").encode(),
-                                      ctypes.byref(self.opt), ctypes.byref(self.ctx)), "create")
+        if physcal_zqp:
+            _check(lib().mvmc_b200_physcal_create(namelist.encode(), physcal_zqp.encode(),
+                                                  ctypes.byref(self.opt), ctypes.byref(self.ctx)), "physcal_create")
+        else:
+            _check(lib().mvmc_b200_create(namelist.encode(), (initial_def or "").encode(),
+                                          ctypes.byref(self.opt), ctypes.byref(self.ctx)), "create")
+        g = (ctypes.c_int * 5)()
+        _check(lib().mvmc_b200_green_dims(self.ctx, g), "green_dims")
+        self.green_dims = dict(zip(["one", "ex", "two", "blocks", "idx_start"], list(g)))
         d = (ctypes.c_int * 8)()
         _check(lib().mvmc_b200_dims(self.ctx, d), "dims")
         keys = ["nsite", "ne", "nqp", "nproj", "npara", "saved", "walkers", "n_orb"]
@@ -191,6 +201,15 @@ class Engine:
         oo = np.zeros(2 * self.sr_size)
         _check(lib().mvmc_b200_measure(self.ctx, _ptr(e), _ptr(ho), _ptr(oo)), "measure")
         return e, ho, oo
+
+    def measure_green(self):
+        """PhysCal measurement: energy[5] (Wc, <E>, <E^2>, <Sz>, <Sz^2>) and the one-body,
+        TwoBodyGEx and TwoBodyG Green functions."""
+        g = self.green_dims
+        e = np.zeros(5)
+        one, ex, two = np.zeros(g["one"]), np.zeros(g["ex"]), np.zeros(g["two"])
+        _check(lib().mvmc_b200_measure_green(self.ctx, _ptr(e), _ptr(one), _ptr(ex), _ptr(two)), "measure_green")
+        return e, one, ex, two
 
     def o_store(self):
         d = self.dims
@@ -282,6 +301,13 @@ def run_opt(namelist, out_dir, initial_def="", nsteps=0, **options):
     opt = default_options(**options)
     _check(lib().mvmc_b200_run_opt(namelist.encode(), (initial_def or "").encode(), out_dir.encode(),
                                    ctypes.byref(opt), nsteps), "run_opt")
+
+
+def run_physcal(namelist, zqp_opt, out_dir, **options):
+    """PhysCal run writing zvo_out_NNN / zvo_var_NNN / zvo_cisajs* files into out_dir."""
+    opt = default_options(**options)
+    _check(lib().mvmc_b200_run_physcal(namelist.encode(), zqp_opt.encode(), out_dir.encode(), ctypes.byref(opt)),
+           "run_physcal")
 
 
 class Stage:

@@ -1685,6 +1685,90 @@ int oracle_physcal_green(const char* namelist, const char* zqp_opt, long long se
   }
 }
 
+int oracle_green_identity(const char* namelist, const char* zqp_opt, long long seed, double* out, char* err,
+                          int err_len) {
+  try {
+    mvmc::Model m = mvmc::read_expert(namelist);
+    std::string why;
+    if (!mvmc::read_para_triples(m, zqp_opt, &why)) throw std::runtime_error("zqp_opt.dat: " + why);
+    mvmc::sync_modified_parameter(m, false);
+    orc::Walker w;
+    w.rng.seed(static_cast<uint32_t>(seed));
+    {
+      mvmc::Model tmp = m;
+      mvmc::init_parameter(tmp, [&]() { return w.rng.real2(); });
+    }
+    if (m.nmp_trans < 0) m.nmp_trans = -m.nmp_trans;
+    mvmc::init_qp_weight(m);
+    std::vector<double> slater;
+    mvmc::build_slater_table(m, slater);
+    orc::Ctx c(m, slater);
+    orc::init_walker(c, w);
+    orc::make_sample(c, w);
+    const int n = c.n, ns = c.ns, ne = c.ne;
+    std::vector<double> inv(static_cast<size_t>(c.nqp) * n * n), pf(c.nqp), inv2(inv.size()), pf2(c.nqp);
+    double worst = 0.0;
+    long long n1 = 0, n2 = 0;
+    // ratio by recomputation: exp(Σ α (c' − c)) · IP(x') / IP(x)
+    auto direct = [&](const std::vector<int64_t>& idx2, const std::vector<int64_t>& num2, const int64_t* cnt,
+                      double ip) {
+      std::vector<int64_t> cnt2(c.nproj);
+      orc::make_proj_cnt(c, num2.data(), cnt2.data());
+      if (orc::calc_m_all(c, idx2.data(), inv2.data(), pf2.data()) != 0) return std::nan("");
+      return std::exp(orc::log_proj_ratio(c, cnt2.data(), cnt)) * orc::ip_of(c, pf2.data()) / ip;
+    };
+    auto note = [&](double a, double b) {
+      if (!std::isfinite(b)) return;
+      worst = std::max(worst, std::fabs(a - b) / std::max(std::fabs(b), 1e-300));
+    };
+    for (int s = 0; s < m.nvmc_sample; ++s) {
+      const int64_t* idx = w.s_idx.data() + static_cast<size_t>(s) * n;
+      const int64_t* cfg = w.s_cfg.data() + static_cast<size_t>(s) * c.ns2;
+      const int64_t* num = w.s_num.data() + static_cast<size_t>(s) * c.ns2;
+      const int64_t* cnt = w.s_cnt.data() + static_cast<size_t>(s) * c.nproj;
+      if (orc::calc_m_all(c, idx, inv.data(), pf.data()) != 0) continue;
+      const double ip = orc::ip_of(c, pf.data());
+      if (std::fabs(ip) < 1.0e-100) continue;
+      const orc::GreenSample gs{idx, cfg, num, cnt, inv.data(), pf.data(), ip};
+      for (const auto& t : m.green_one) {
+        if (t.si != t.sj || t.i == t.j) continue;
+        const int dst = t.i + t.si * ns, src = t.j + t.sj * ns;
+        if (num[dst] == 1 || num[src] == 0) continue;
+        std::vector<int64_t> idx2(idx, idx + n), num2(num, num + c.ns2);
+        idx2[cfg[src] + t.sj * ne] = t.i;
+        num2[dst] = 1;
+        num2[src] = 0;
+        note(orc::green_one(c, gs, t.i, t.j, t.si, t.sj), direct(idx2, num2, cnt, ip));
+        ++n1;
+      }
+      for (const auto& t : m.green_two) {
+        const int ri = t.i, rj = t.j, rk = t.k, rl = t.l, sp = t.si, u = t.sk;
+        const bool coincident = sp == u ? (rk == rl || rj == rl || ri == rl || rj == rk || ri == rk || ri == rj)
+                                        : (rk == rl || ri == rj);
+        if (coincident) continue;
+        if (num[ri + sp * ns] != 0 || num[rj + sp * ns] != 1 || num[rk + u * ns] != 0 || num[rl + u * ns] != 1)
+          continue;
+        std::vector<int64_t> idx2(idx, idx + n), num2(num, num + c.ns2);
+        idx2[cfg[rl + u * ns] + u * ne] = rk;
+        idx2[cfg[rj + sp * ns] + sp * ne] = ri;
+        num2[rl + u * ns] = 0;
+        num2[rk + u * ns] = 1;
+        num2[rj + sp * ns] = 0;
+        num2[ri + sp * ns] = 1;
+        note(orc::green_two(c, gs, ri, rj, rk, rl, sp, u), direct(idx2, num2, cnt, ip));
+        ++n2;
+      }
+    }
+    out[0] = worst;
+    out[1] = static_cast<double>(n1);
+    out[2] = static_cast<double>(n2);
+    return 0;
+  } catch (const std::exception& e) {
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
+}
+
 int oracle_opt_step1_walkers(const char* namelist, const char* initial_def, int walkers,
                              long long seed, int64_t* ele_idx, int64_t* proj_cnt, int64_t* counters,
                              int64_t* draws, double* energy, double* ho, double* oo, double* ostore,

@@ -67,6 +67,14 @@ int oracle_physcal_green(const char* namelist, const char* zqp_opt, long long se
                          double* energy, double* one, double* ex, double* two, const char* out_dir,
                          char* err, int err_len);
 
+// Identity check of the Green-function ratios: one PhysCal block on one chain; for every
+// valid sample and every one-body hop and general (two-hop) TwoBodyG term whose moves are
+// allowed, the update-formula ratio against exp(Σ α Δc)·IP(x')/IP(x) with IP(x') from a
+// fresh CalculateMAll of the moved configuration. out[0] = largest relative difference,
+// out[1] = number of one-body hops checked, out[2] = number of two-hop terms checked.
+int oracle_green_identity(const char* namelist, const char* zqp_opt, long long seed, double* out, char* err,
+                          int err_len);
+
 // Step 1 of an optimisation with W chains (seed + w): every walker's saved samples,
 // counters, draw counts, the O store [W][S][sr_size] and the reduced operands
 // (energy[5] = Wc, <E>, <E^2>, <Sz>, <Sz^2>; ho[sr_size]; oo[2*sr_size]).

@@ -180,3 +180,11 @@ def cholesky_solve(a, b):
     b = np.ascontiguousarray(b, dtype=np.float64).copy()
     info = lib().oracle_cholesky_solve(ptr(a), ptr(b), len(b))
     return info, b
+
+
+def green_identity(namelist, zqp, seed=1):
+    out = np.zeros(3)
+    err = err_buf()
+    if lib().oracle_green_identity(namelist.encode(), zqp.encode(), ctypes.c_longlong(seed), ptr(out), err, 1024) != 0:
+        raise RuntimeError(err.value.decode())
+    return out

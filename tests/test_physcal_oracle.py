@@ -47,3 +47,30 @@ def test_physcal_files_have_the_c_layout(tmp_path):
                         assert abs(float(x) - float(y)) <= max(1e-13, 1e-10 * abs(float(y))), (name, x, y)
                     else:
                         assert x == y, (name, a, b)
+
+
+def test_green_ratios_match_recomputed_amplitudes(tmp_path):
+    """The one-electron and two-hop ratios of the Green functions against exp(Σ α Δc)·
+    IP(x')/IP(x) with IP(x') from a fresh CalculateMAll of every moved configuration
+    (the fixture's TwoBodyG list has no general two-hop term; this list reaches them)."""
+    from mvmc_lib import green_term_mix, write_green_lists
+    one, two, ex = green_term_mix(6, np.random.default_rng(3))
+    nl = write_green_lists(os.path.join(D, "inputs"), str(tmp_path / "in"), one, two, ex)
+    worst, n1, n2 = ol.green_identity(nl, ZQP)
+    assert n1 > 1000 and n2 > 1000, (n1, n2)
+    assert worst < 1e-11, worst
+
+
+def test_two_body_ex_canonical_map(tmp_path):
+    """OneBodyG is de-duplicated when TwoBodyGEx is present, and the factors that it lacks
+    are appended in TwoBodyGEx order (types.rs:1169-1215)."""
+    from mvmc_lib import write_green_lists
+    one = [(0, 0, 1, 0), (0, 0, 1, 0), (2, 1, 3, 1)]
+    ex = [(0, 0, 1, 0, 4, 1, 5, 1), (2, 1, 3, 1, 0, 0, 1, 0)]
+    nl = write_green_lists(os.path.join(D, "inputs"), str(tmp_path / "in"), one, [], ex)
+    g = ol.green_dims(nl)
+    # (0 0 1 0), (2 1 3 1), then (5 1 4 1) and (1 0 0 0) from the factored terms
+    assert (g["one"], g["ex"], g["two"]) == (4, 2, 0)
+    ol.physcal_green(nl, ZQP, 1, 1, out_dir=str(tmp_path))
+    rows = [line.split()[:4] for line in open(tmp_path / "zvo_cisajs_007.dat") if line.strip()]
+    assert rows == [["0", "0", "1", "0"], ["2", "1", "3", "1"], ["5", "1", "4", "1"], ["1", "0", "0", "0"]]

@@ -12,6 +12,11 @@ updates, FP64 refresh every --refresh sweeps and after guard-tripping moves) is 
 beside it on the same workload and seeds (`mixed_path`), and `accuracy` compares one
 fresh sample + measurement of the two.
 
+PhysCal workload (physcal8): the square8 model with fixed parameters; a step is one data
+block — resident sampling of one sample per walker, then the measurement in the PhysCal
+form: energy plus the one-body Green function of every same-spin site pair and the
+density-density function of every site pair (8192 + 16384 terms); `value` is samples/s.
+
 Pfaffian workloads (pfinv64, pfinv_mix): a step is one batched Pfaffian + inverse launch
 over B = 8192 (8190 for the five-size mix) seeded skew planes; `value` is planes/s.
 
@@ -43,6 +48,8 @@ METRIC = "Metropolis sweeps/s & SR-step time: mixed vs FP64 path on 1 B200 at |d
 # 296 walkers x 4 sweeps), scaled to a launch by walker-sweeps.
 SAMPLE_DRAM_PER_WALKER_SWEEP = {("square8", 64): 2.632e9 / (296 * 4)}
 PFINV_METRIC = "Pfaffian+inverse/s (batched skew FP64)"
+PHYSCAL = {"physcal8": 4096}
+PHYSCAL_METRIC = "PhysCal samples/s (energy + one- and two-body Green functions, FP64)"
 
 
 def measured_peaks():
@@ -423,6 +430,152 @@ def engine_bench(args, ws, rank, local):
 
 
 # ----------------------------------------------------------------------------------------
+# PhysCal workload.
+# ----------------------------------------------------------------------------------------
+def _physcal_job(args):
+    namelist, zqp, walkers, seed = args
+    _oracle_lib().physcal_green(namelist, zqp, seed, walkers)
+    return 0
+
+
+def physcal_flops(dims, nterm_one, samples):
+    """Algorithmic FP64 flops of the PhysCal measurement of the given samples: per QP plane
+    the Pfaffian + inverse (2n³) and 2n per allowed one-body hop (same spin, destination
+    empty, source occupied), from the terms (i, s, j, t) of the one-body list."""
+    n, nqp, ns = dims["n"], dims["nqp"], dims["nsite"]
+    num = samples["ele_num"].reshape(-1, 2 * ns)
+    occ_up, occ_dn = num[:, :ns].sum(axis=1), num[:, ns:].sum(axis=1)
+    # the list holds every same-spin pair (i, j), so the allowed hops are empty × occupied
+    hops = (ns - occ_up) * occ_up + (ns - occ_dn) * occ_dn
+    assert nterm_one == 2 * ns * ns
+    return float(np.sum(nqp * (2.0 * n ** 3 + 2.0 * n * hops)))
+
+
+def reference_physcal(args):
+    cfg, tmp, namelist, initial_def, dims = engine_inputs(args, 0)
+    procs = os.cpu_count() or 1
+    per = 2
+    pool = CpuPool(procs, initializer=_oracle_lib)
+    jobs = [(namelist, initial_def, per, 12345 + k * per) for k in range(procs)]
+    for _ in range(args.warmup):
+        pool.time(_physcal_job, jobs)
+    times = [pool.time(_physcal_job, jobs) for _ in range(args.steps)]
+    pool.close()
+    t = sum(times) / len(times)
+    value = procs * per * cfg["samples"] / t
+    return {"metric": PHYSCAL_METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config, "walkers": procs * per},
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": procs, "kind": "port",
+                             "sample": f"{procs * per} chains x one PhysCal block (warm-up + {cfg['samples']} "
+                                       f"sample) of {args.config}, one process per core"},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def physcal_bench(args, ws, rank, local):
+    import torch
+    import mvmc_b200 as mb
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    cfg, tmp, namelist, initial_def, dims = engine_inputs(args, rank)
+    W = args.walkers or PHYSCAL[args.config]
+    S = cfg["samples"]
+    eng = mb.Engine(namelist, physcal_zqp=initial_def, walkers=W, precision=64, seed=12345 + rank * W, device=local)
+    stream = torch.cuda.ExternalStream(eng.stream())
+
+    def block():
+        eng.sample()
+        e, one, ex, two = eng.measure_green()
+        if ws > 1:
+            # chains on other GPUs: energy sums and the per-rank averaged Green functions
+            sums = np.concatenate([[e[0]], e[1:] * e[0]])
+            t = torch.as_tensor(np.concatenate([sums, one, ex, two]), device="cuda")
+            dist.all_reduce(t)
+            t = t.cpu().numpy()
+            e = np.concatenate([[t[0]], t[1:5] / t[0]])
+            one = t[5:5 + len(one)] / ws
+        return e, one
+
+    for _ in range(args.warmup):
+        block()
+    torch.cuda.synchronize()
+    clocks_path = os.path.join(tmp, "clocks.csv")
+    sampler = start_clock_sampler(clocks_path) if rank == 0 else None
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    h0, d0 = eng.transfer_bytes()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    marks = []
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    flops = 0.0
+    for _ in range(args.steps):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record(stream)
+        eng.sample()
+        b.record(stream)
+        e, one, ex, two = eng.measure_green()
+        c.record(stream)
+        marks.append((a, b, c))
+        energy = float(e[1])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t0
+    stop_clock_sampler(sampler)
+    h1, d1 = eng.transfer_bytes()
+    ms = ev0.elapsed_time(ev1)
+    if ws > 1:
+        t = torch.tensor([ms, t_wall * 1e3], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, t_wall = float(t[0]), float(t[1]) / 1e3
+    samp = [a.elapsed_time(b) for a, b, _ in marks]
+    meas = [b.elapsed_time(c) for _, b, c in marks]
+    flops = physcal_flops(dims, eng.green_dims["one"], eng.samples())
+    eng.close()
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return
+    total = ws * W * S * args.steps
+    meas_ms = sum(meas) / len(meas)
+    achieved = flops / (meas_ms / 1e3) / 1e12
+    peak = fp64_gemm_peak()
+    _oracle_lib()
+    t_cpu = time.perf_counter()
+    _physcal_job((namelist, initial_def, 2, 12345))
+    t_cpu = time.perf_counter() - t_cpu
+    out = {
+        "metric": PHYSCAL_METRIC, "value": total / (ms / 1e3), "unit": "samples/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, "walkers_per_gpu": W, "samples_per_walker": S, "nsite": dims["nsite"],
+                   "n": dims["n"], "nqp": dims["nqp"], "green_one": eng.green_dims["one"],
+                   "green_two": eng.green_dims["two"], "parallelism": f"walker-sharded{ws}" if ws > 1 else "1",
+                   "l2": "inputs larger than L2 between steps (walker planes and Green rows)"},
+        "sample_ms": sum(samp) / len(samp), "measure_ms": meas_ms, "energy": energy,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_measure (PhysCal form)",
+                     "peak_kind": "measured cuBLAS FP64 GEMM on this GPU",
+                     "algorithmic_flops_per_launch": flops},
+        "cpu_baseline": {"value": 2 * S / t_cpu, "unit": "samples/s", "cores": 1, "kind": "port",
+                         "sample": f"2 chains x one PhysCal block (warm-up + {S} sample) of {args.config}"},
+        "e2e": {"value": total / t_wall, "unit": "samples/s", "h2d_bytes_per_step": (h1 - h0) // args.steps,
+                "d2h_bytes_per_step": (d1 - d0) // args.steps},
+        "gpu_launches": 6 * args.steps,
+        "clocks": summarize_clocks(clocks_path, local),
+    }
+    print(json.dumps(out), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------------------
 # Pfaffian workloads.
 # ----------------------------------------------------------------------------------------
 def fp64_gemm_peak():
@@ -570,7 +723,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="square8", choices=sorted(WALKERS) + sorted(PFINV))
+    ap.add_argument("--config", default="square8", choices=sorted(WALKERS) + sorted(PFINV) + sorted(PHYSCAL))
     ap.add_argument("--precision", type=int, default=64, choices=(32, 64),
                     help="64: plain FP64 path (default); 32: mixed path (FP32 inverses, FP64 refresh)")
     ap.add_argument("--walkers", type=int, default=0)
@@ -587,13 +740,17 @@ def main():
     args = ap.parse_args()
     ws, rank, local = dist_env()
     pf = args.config in PFINV
+    pc = args.config in PHYSCAL
     if args.impl == "reference":
         if rank != 0:
             return
-        print(json.dumps(reference_pfinv(args) if pf else reference_engine(args)), flush=True)
+        ref = reference_pfinv(args) if pf else (reference_physcal(args) if pc else reference_engine(args))
+        print(json.dumps(ref), flush=True)
         return
     if pf:
         pfinv_bench(args, ws, rank, local)
+    elif pc:
+        physcal_bench(args, ws, rank, local)
     else:
         engine_bench(args, ws, rank, local)
 

@@ -25,7 +25,8 @@ int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const 
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
                    double* eloc, double* lpsi, int* valid, double* gval, unsigned* status, cudaStream_t stream);
 int launch_green_reduce(const DevModel& m, int W, int S, int n_one, int nex, const int* ex, const double* gval,
-                        const int* valid, double* out, cudaStream_t stream);
+                        const int* valid, double* part, double* out, cudaStream_t stream);
+int green_chunks(int W);
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,
                   const int* valid, const int* s_num, double* wsum, double* tot, cudaStream_t stream);
 int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
@@ -144,6 +145,7 @@ struct mvmc_b200_ctx {
   size_t gval_cap = 0;
   int* d_gex = nullptr;
   double* d_gout = nullptr;
+  double* d_gpart = nullptr;  // [chunks][outputs] walker-chunk partial sums
   int n_one = 0, n_ex = 0;
   std::vector<double> tot;  // host copy of the last reduction
   long long h2d = 0, d2h = 0;  // bytes copied across the host boundary
@@ -254,6 +256,28 @@ void build_green_tables(mvmc_b200_ctx* c) {
   }
   std::vector<int> gone, gex;
   for (const auto& t : one) gone.insert(gone.end(), {t.i, t.si, t.j, t.sj});
+  // dense one-body lists (at least half of the Ns² same-spin pairs of a spin on average):
+  // the per-plane product over all (empty site, electron) pairs
+  const int ns = m.nsite;
+  std::vector<int> term_of(2 * static_cast<size_t>(ns) * ns, -1), first(one.size());
+  int distinct = 0;
+  for (size_t k = 0; k < one.size(); ++k) {
+    const auto& t = one[k];
+    first[k] = static_cast<int>(k);
+    if (t.si != t.sj || t.i == t.j) continue;
+    int& slot = term_of[(static_cast<size_t>(t.si) * ns + t.i) * ns + t.j];
+    if (slot < 0) {
+      slot = static_cast<int>(k);
+      ++distinct;
+    } else {
+      first[k] = slot;
+    }
+  }
+  DevModel& dmg = c->dm;
+  dmg.gdense = 2 * distinct >= ns * ns ? 1 : 0;
+  if (const char* f = std::getenv("MVMC_B200_GREEN_DENSE")) dmg.gdense = std::atoi(f) != 0 ? 1 : 0;
+  dmg.gterm_of = c->upload(term_of);
+  dmg.gfirst = c->upload(first);
   for (const auto& p : m.green_two_ex) gex.insert(gex.end(), {p.first, p.second});
   DevModel& dm = c->dm;
   dm.ngone = static_cast<int>(one.size());
@@ -267,6 +291,7 @@ void build_green_tables(mvmc_b200_ctx* c) {
   c->n_one = static_cast<int>(m.green_one.size());
   c->n_ex = static_cast<int>(m.green_two_ex.size());
   c->d_gout = c->alloc<double>(c->n_one + c->n_ex + dm.ngtwo);
+  c->d_gpart = c->alloc<double>(static_cast<size_t>(green_chunks(c->W)) * (c->n_one + c->n_ex + dm.ngtwo));
 }
 
 // physcal_zqp (PhysCal, prepare_phys_cal_from_namelist run.rs:555-737): every walker still
@@ -499,8 +524,8 @@ int do_measure_green(mvmc_b200_ctx* c, std::vector<double>& gout) {
   rc = launch_reduce(energy_only, c->W, c->S, nullptr, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
                      c->stream);
   if (rc != kOk) return rc;
-  rc = launch_green_reduce(c->dm, c->W, c->S, c->n_one, c->n_ex, c->d_gex, c->d_gval, c->d_valid, c->d_gout,
-                           c->stream);
+  rc = launch_green_reduce(c->dm, c->W, c->S, c->n_one, c->n_ex, c->d_gex, c->d_gval, c->d_valid, c->d_gpart,
+                           c->d_gout, c->stream);
   if (rc != kOk) return rc;
   c->tot.assign(5, 0.0);
   check(cudaMemcpyAsync(c->tot.data(), c->d_tot, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream),

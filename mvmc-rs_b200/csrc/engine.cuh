@@ -41,6 +41,13 @@ struct DevModel {
   // of that one-body value (ref, or -1) and of their two-hop slot (gen, or -1). A measured
   // sample's row holds [ngone one-body | ngtwo two-body | nggen two-hop] values (width gw).
   int ngone = 0, ngtwo = 0, nggen = 0, gw = 0;
+  int gacc_smem = 0;          // set by the launcher: one-body plane sums in shared memory
+  // Dense one-body lists: all (empty destination, electron) pairs of a spin are evaluated
+  // as one product per plane; gterm_of[(s·ns + i)·ns + j] = first one-body term
+  // (i s j s) with i != j (or -1), gfirst[k] = first term equal to term k.
+  int gdense = 0;
+  const int* gterm_of = nullptr;
+  const int* gfirst = nullptr;
   const int* gone = nullptr;  // [ngone*4]: i, s, j, t of c†_{i s} c_{j t}
   const int* gtwo = nullptr;  // [ngtwo*8]: ri, rj, rk, rl, s, u, ref, gen
   const int* ggen = nullptr;  // [nggen*6]: ri, rj, rk, rl, s, u of the two-hop terms

@@ -23,6 +23,8 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
+#include <cstring>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -31,9 +33,12 @@
 namespace mvmcb {
 
 constexpr int kMeasThreads = 256;
+// dense one-body product: destination rows per tile (warps × rows per thread)
+constexpr int kGreenRows = 4;
+constexpr int kGreenTile = (kMeasThreads / 32) * kGreenRows;
 
 struct MeasLayout {
-  size_t idx, cfg, num, cnt, tr, sg, pf, tacc, g1, oacc, cj, gscr, gj, plane, total;
+  size_t idx, cfg, num, cnt, tr, sg, pf, tacc, g1, oacc, cj, gscr, gacc, gempty, gtile, gj, plane, total;
 };
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -55,6 +60,14 @@ __host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_p
   // two-hop scratch: the gathered Slater rows u, v of one term per warp
   L.gscr = o;
   if (green && m.nggen > 0) o = a16(o + sizeof(double) * 2 * (kMeasThreads / 32) * static_cast<size_t>(m.n));
+  // one-body plane sums (when they fit beside the planes)
+  L.gacc = o;
+  if (green && m.gacc_smem) o = a16(o + sizeof(double) * static_cast<size_t>(m.ngone));
+  // dense one-body product: the empty sites of each spin and one tile of gathered rows
+  L.gempty = o;
+  if (green && m.gdense) o = a16(o + sizeof(int) * 2 * static_cast<size_t>(m.ns));
+  L.gtile = o;
+  if (green && m.gdense) o = a16(o + sizeof(double) * kGreenTile * static_cast<size_t>(m.n));
   L.gj = o;
   L.plane = o;
   // the plane and its ping-pong partner
@@ -81,6 +94,25 @@ __device__ double hop_log_proj(const DevModel& m, int src, int dst, Occ occ) {
   return z;
 }
 
+// Σ_k α_k Δc_k of the hop src → dst (spin-site slots src_slot, dst_slot) from the
+// charges before the move and cj[r] = Σ_site J(r, site)·(n_site − 1): the O(1) form of
+// calh1_direct_projection_ratio_moved (observables.rs:1680-1758).
+__device__ inline double direct_hop_log_proj(const DevModel& m, const int* num, const double* cj, int source,
+                                             int dest, int src_slot, int dst_slot) {
+  const int ns = m.ns;
+  auto occ = [&](int slot) { return slot == src_slot ? 0 : (slot == dst_slot ? 1 : num[slot]); };
+  auto chm = [&](int site) { return occ(site) + occ(ns + site) - 1; };
+  auto ch = [&](int site) { return num[site] + num[ns + site] - 1; };
+  double z = 0.0;
+  z -= m.gutz_site[source] * static_cast<double>(occ(source) + occ(ns + source));
+  z += m.gutz_site[dest] * static_cast<double>(occ(dest) * occ(ns + dest));
+  const double jsd = m.jast_pair[source * ns + dest];
+  z += jsd * static_cast<double>(chm(source) - chm(dest) + 1);
+  const double sum_dest = cj[dest] - m.jast_pair[dest * ns + source] * static_cast<double>(ch(source));
+  const double sum_src = cj[source] - m.jast_pair[source * ns + dest] * static_cast<double>(ch(dest));
+  return z + (sum_dest - sum_src);
+}
+
 // Julia's complex quotient (pfapack julia_complex.rs:9-75) for a real numerator a and a
 // real denominator c: a·(1/c), rescaled by powers of two when |a| or |c| is extreme.
 __device__ inline double julia_real_quotient(double a, double c) {
@@ -99,28 +131,102 @@ __device__ inline double julia_real_quotient(double a, double c) {
   return a * t * s;
 }
 
+// Dense one-body product on one plane: for every spin s, every empty site r of spin s and
+// every electron m of spin s, R = Σ_k F(r, r_k)·X⁻¹[m][k] with r_k the electron sites, read
+// as −Σ_k F(r, r_k)·X⁻¹[k][m] (X⁻¹ is skew) so that lanes take consecutive m; the moved
+// electron's own term is corrected to F(r, r)·X⁻¹[m][m] (calculate_new_pf_m2_real_flat with
+// the configuration after the hop). Pf' = −Pf·R is added to the one-body term (r s j s), j
+// the site of m. Rows are tiled kGreenTile at a time through shared memory.
+__device__ void green_dense_plane(const DevModel& m, int q, double wq, double pfv, const double* A, const int* idx,
+                                  const int* gempty, double* gtile, double* gacc) {
+  const int n = m.n, ns = m.ns, ne = m.ne, ns2 = m.ns2, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int ce = ns - ne;  // empty sites per spin
+  const double* slq = m.slater + static_cast<size_t>(q) * ns2 * ns2;
+  for (int s = 0; s < 2; ++s) {
+    const int* empty = gempty + s * ns;
+    for (int r0 = 0; r0 < ce; r0 += kGreenTile) {
+      const int rows = min(kGreenTile, ce - r0);
+      for (int k = tid; k < rows * n; k += nt) {
+        const int rr = k / n, c = k - rr * n;
+        const int rs = empty[r0 + rr] + s * ns;
+        gtile[k] = __ldg(slq + static_cast<size_t>(rs) * ns2 + idx[c] + (c >= ne ? ns : 0));
+      }
+      __syncthreads();
+      for (int e0 = 0; e0 < ne; e0 += 32) {
+        const int e = e0 + lane;
+        const int mcol = s * ne + min(e, ne - 1);
+        double acc[kGreenRows];
+#pragma unroll
+        for (int i = 0; i < kGreenRows; ++i) acc[i] = 0.0;
+        const double* g0 = gtile + static_cast<size_t>(warp * kGreenRows) * n;
+        for (int k = 0; k < n; ++k) {
+          const double a = A[static_cast<size_t>(k) * n + mcol];
+#pragma unroll
+          for (int i = 0; i < kGreenRows; ++i) acc[i] += g0[i * n + k] * a;
+        }
+        if (e < ne) {
+          const int msj = s * ne + e;
+          const int site_j = idx[msj];
+          const double amm = A[static_cast<size_t>(msj) * n + msj];
+#pragma unroll
+          for (int i = 0; i < kGreenRows; ++i) {
+            const int rr = warp * kGreenRows + i;
+            if (rr >= rows) continue;
+            const int site_i = empty[r0 + rr];
+            const int t = m.gterm_of[(s * ns + site_i) * ns + site_j];
+            if (t < 0) continue;
+            const int rs = site_i + s * ns;
+            // R over rows m: −acc; the moved electron's slot holds F(r, r) instead of F(r, r_m)
+            const double r = -acc[i] + amm * (__ldg(slq + static_cast<size_t>(rs) * ns2 + rs) -
+                                              __ldg(slq + static_cast<size_t>(rs) * ns2 + site_j + s * ns));
+            gacc[t] += wq * (-r * pfv);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // Per-plane Green contributions of one sample: Σ_q w_q·Pf'_q of every one-body hop and of
 // every two-hop term, added into the sample's row (plane order).
 template <int JPL>
 __device__ void green_plane(const DevModel& m, int q, double wq, double pfv, const double* A, const int* idx,
-                            const int* cfg, const int* num, double* grow, double* gscr) {
+                            const int* cfg, const int* num, double* gacc, double* grow, double* gscr) {
   const int n = m.n, ns = m.ns, ne = m.ne, lane = threadIdx.x & 31, warp = threadIdx.x >> 5,
             nwarp = blockDim.x >> 5;
-  // one-body: the electron at rj (spin t) moves to the empty ri: Pf' = −Pf·Σ_k X⁻¹[msj][k]·F(ri, r'_k)
-  for (int k = warp; k < m.ngone; k += nwarp) {
-    const int gi = m.gone[4 * k], gs = m.gone[4 * k + 1], gj = m.gone[4 * k + 2], gt = m.gone[4 * k + 3];
-    const int dst = gi + gs * ns, src = gj + gt * ns;
-    if (gs != gt || gi == gj || num[dst] == 1 || num[src] == 0 || cfg[src] < 0) continue;
-    const int msj = cfg[src] + gt * ne;
-    const double* row = A + static_cast<size_t>(msj) * n;
-    const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + (gi + gt * ns)) * m.ns2;
-    double r = 0.0;
-    for (int c = lane; c < n; c += 32) {
-      const int rc = (c == msj ? gi : idx[c]) + (c >= ne ? ns : 0);
-      r += row[c] * __ldg(srow + rc);
+  // one-body: the electron at rj (spin t) moves to the empty ri: Pf' = −Pf·Σ_k X⁻¹[msj][k]·F(ri, r'_k).
+  // Each warp tests 32 terms at once (one per lane) and runs the allowed ones in turn.
+  for (int base = warp * 32; base < (m.gdense ? 0 : m.ngone); base += nwarp * 32) {
+    const int k = base + lane;
+    bool allowed = false;
+    int gi = 0, gt = 0, msj = 0;
+    if (k < m.ngone) {
+      const int4 term = __ldg(reinterpret_cast<const int4*>(m.gone) + k);
+      gi = term.x;
+      const int gs = term.y, gj = term.z;
+      gt = term.w;
+      const int dst = gi + gs * ns, src = gj + gt * ns;
+      allowed = gs == gt && gi != gj && num[dst] == 0 && num[src] == 1 && cfg[src] >= 0;
+      if (allowed) msj = cfg[src] + gt * ne;
     }
-    r = warp_sum(r);
-    if (lane == 0) grow[k] += wq * (-r * pfv);
+    unsigned todo = __ballot_sync(0xffffffffu, allowed);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int ti = __shfl_sync(0xffffffffu, gi, j), tt = __shfl_sync(0xffffffffu, gt, j);
+      const int tm = __shfl_sync(0xffffffffu, msj, j);
+      const double* row = A + static_cast<size_t>(tm) * n;
+      const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + (ti + tt * ns)) * m.ns2;
+      double r = 0.0;
+      for (int c = lane; c < n; c += 32) {
+        const int rc = (c == tm ? ti : idx[c]) + (c >= ne ? ns : 0);
+        r += row[c] * __ldg(srow + rc);
+      }
+      r = warp_sum(r);
+      if (lane == j) gacc[k] += wq * (-r * pfv);
+    }
   }
   // two-hop: electron msa moves rl → rk (spin u), then msb moves rj → ri (spin s);
   // ratio = X_ab·v_a + X_ab·(vᵀ X u) + p_a q_b − p_b q_a with u, v the moved rows
@@ -171,18 +277,20 @@ __device__ void green_plane(const DevModel& m, int q, double wq, double pfv, con
 }
 
 // Final Green values of one sample from the plane sums (run after the energy, all threads).
-__device__ void green_finish(const DevModel& m, double ip, bool ok, const int* cfg, const int* num, double* grow) {
+__device__ void green_finish(const DevModel& m, double ip, bool ok, const int* cfg, const int* num, const double* cj,
+                             const double* gacc, double* grow) {
   const int ns = m.ns, tid = threadIdx.x, nt = blockDim.x;
   for (int k = tid; k < m.ngone; k += nt) {
-    const int gi = m.gone[4 * k], gs = m.gone[4 * k + 1], gj = m.gone[4 * k + 2], gt = m.gone[4 * k + 3];
+    const int4 term = __ldg(reinterpret_cast<const int4*>(m.gone) + k);
+    const int gi = term.x, gs = term.y, gj = term.z, gt = term.w;
     const int dst = gi + gs * ns, src = gj + gt * ns;
     double v;
     if (ip == 0.0) v = 0.0;
     else if (gs == gt && gi == gj) v = static_cast<double>(num[src]);
     else if (gs != gt || num[dst] == 1 || num[src] == 0 || cfg[src] < 0) v = 0.0;
     else {
-      auto occ = [&](int slot) { return slot == src ? 0 : (slot == dst ? 1 : num[slot]); };
-      v = julia_real_quotient(exp(hop_log_proj(m, gj, gi, occ)) * grow[k], ip);
+      const double a = gacc[m.gdense ? m.gfirst[k] : k];
+      v = julia_real_quotient(exp(direct_hop_log_proj(m, num, cj, gj, gi, src, dst)) * a, ip);
     }
     grow[k] = ok ? v : 0.0;
   }
@@ -204,8 +312,9 @@ __device__ void green_finish(const DevModel& m, double ip, bool ok, const int* c
   const double* one = grow;
   const double* gen = grow + m.ngone + m.ngtwo;
   for (int k = tid; k < m.ngtwo; k += nt) {
-    const int* t = m.gtwo + 8 * k;
-    const int ri = t[0], rj = t[1], rk = t[2], rl = t[3], s = t[4], u = t[5], ref = t[6], gi = t[7];
+    const int4 t0 = __ldg(reinterpret_cast<const int4*>(m.gtwo) + 2 * k);
+    const int4 t1 = __ldg(reinterpret_cast<const int4*>(m.gtwo) + 2 * k + 1);
+    const int ri = t0.x, rj = t0.y, rk = t0.z, rl = t0.w, s = t1.x, u = t1.y, ref = t1.z, gi = t1.w;
     const int rsi = ri + s * ns, rsj = rj + s * ns, rtk = rk + u * ns;
     double v;
     if (s == u) {
@@ -265,8 +374,14 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
     for (int k = tid; k < m.nterm; k += nt) tacc[k] = 0.0;
     for (int k = tid; k < m.norb; k += nt) oacc[k] = 0.0;
     double* grow = kGreen ? gval + static_cast<size_t>(sample) * m.gw : nullptr;
-    if (kGreen)
+    double* gacc = kGreen && m.gacc_smem ? reinterpret_cast<double*>(smem + L.gacc) : grow;
+    int* gempty = reinterpret_cast<int*>(smem + L.gempty);
+    double* gtile = reinterpret_cast<double*>(smem + L.gtile);
+    if (kGreen) {
       for (int k = tid; k < m.gw; k += nt) grow[k] = 0.0;
+      if (m.gacc_smem)
+        for (int k = tid; k < m.ngone; k += nt) gacc[k] = 0.0;
+    }
     if (tid == 0) s_bad = 0;
     __syncthreads();
     // direct projection helper: cj[r] = Σ_site J[r][site]·(n_site − 1)
@@ -275,6 +390,17 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
       for (int site = 0; site < ns; ++site)
         acc += __ldg(m.jast_pair + r * ns + site) * static_cast<double>(num[site] + num[site + ns] - 1);
       cj[r] = acc;
+    }
+    if (kGreen && m.gdense && warp < 2) {
+      // empty sites of spin `warp`, in site order (ballot prefix over 32 sites at a time)
+      int count = 0;
+      for (int b = 0; b < ns; b += 32) {
+        const int site = b + lane;
+        const bool e = site < ns && s_num[static_cast<size_t>(sample) * m.ns2 + site + warp * ns] == 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, e);
+        if (e) gempty[warp * ns + count + __popc(mask & ((1u << lane) - 1u))] = site;
+        count += __popc(mask);
+      }
     }
     if (tid == 0) {
       bool all_zero = true, all_neg = true;
@@ -332,7 +458,8 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
         if (lane == 0) tacc[t] += wq * (-r * pfv);
       }
       if (kGreen) {
-        green_plane<JPL>(m, q, wq, pfv, A, idx, cfg, num, grow, gscr);
+        if (m.gdense) green_dense_plane(m, q, wq, pfv, A, idx, gempty, gtile, gacc);
+        green_plane<JPL>(m, q, wq, pfv, A, idx, cfg, num, gacc, grow, gscr);
         __syncthreads();
         continue;  // PhysCal: no O row
       }
@@ -384,18 +511,7 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
         g = 0.0;
       } else {
         // calh1_direct_projection_ratio_moved: source = tj, dest = ti, spin tsj
-        const int source = tj, dest = ti;
-        auto occ = [&](int slot) { return slot == src ? 0 : (slot == dst ? 1 : num[slot]); };
-        auto chm = [&](int site) { return occ(site) + occ(ns + site) - 1; };
-        auto ch = [&](int site) { return num[site] + num[ns + site] - 1; };
-        double z = 0.0;
-        z -= m.gutz_site[source] * static_cast<double>(occ(source) + occ(ns + source));
-        z += m.gutz_site[dest] * static_cast<double>(occ(dest) * occ(ns + dest));
-        const double jsd = m.jast_pair[source * ns + dest];
-        z += jsd * static_cast<double>(chm(source) - chm(dest) + 1);
-        const double sum_dest = cj[dest] - m.jast_pair[dest * ns + source] * static_cast<double>(ch(source));
-        const double sum_src = cj[source] - m.jast_pair[source * ns + dest] * static_cast<double>(ch(dest));
-        z += sum_dest - sum_src;
+        const double z = direct_hop_log_proj(m, num, cj, tj, ti, src, dst);
         g = exp(z) * tacc[t] / ip;
       }
       g1[t] = g;
@@ -431,7 +547,7 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
     __syncthreads();
     const bool ok = pf[m.nqp + 1] != 0.0;
     if (kGreen) {
-      green_finish(m, ip, ok, cfg, num, grow);
+      green_finish(m, ip, ok, cfg, num, cj, gacc, grow);
       continue;
     }
     const double inv_ip = ip / (ip * ip);
@@ -511,9 +627,31 @@ __global__ void k_weight_average(int size, double* tot) {
 size_t measure_smem(const DevModel& m, bool smem_plane) { return meas_layout(m, smem_plane).total; }
 
 template <int JPL, bool kGreen>
-int launch_measure_kind(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num, const int* s_cnt,
+int launch_measure_kind(const DevModel& m_in, const int* s_idx, const int* s_cfg, const int* s_num, const int* s_cnt,
                         int nsamples, double* gws, int gws_blocks, double* ostore, double* eloc, double* lpsi,
                         int* valid, double* gval, unsigned* status, cudaStream_t stream, int limit) {
+  DevModel m = m_in;
+  // one-body plane sums in shared memory when they fit beside the layout (planes in shared
+  // memory if those fit too)
+  m.gacc_smem = 0;
+  if (kGreen) {
+    // One-body plane sums in shared memory only when that costs no co-resident sample: the
+    // measurement is latency bound, and two samples per SM with the sums in the L2-resident
+    // row beat one sample per SM with them in shared memory (24.8 → 14.6 ms at 2D 8×8 with
+    // the 8192-term list). MVMC_B200_GREEN_ACC=smem|global overrides.
+    auto per_sm = [&](bool acc) {
+      DevModel t = m;
+      t.gacc_smem = acc ? 1 : 0;
+      size_t total = meas_layout(t, true, true).total;
+      if (total > static_cast<size_t>(limit)) total = meas_layout(t, false, true).total;
+      return total > static_cast<size_t>(limit) ? 0 : static_cast<int>((limit + 1024) / (total + 1024));
+    };
+    m.gacc_smem = per_sm(true) >= per_sm(false) && per_sm(true) > 0 ? 1 : 0;
+    if (const char* e = std::getenv("MVMC_B200_GREEN_ACC")) {
+      if (std::strcmp(e, "global") == 0) m.gacc_smem = 0;
+      if (std::strcmp(e, "smem") == 0 && per_sm(true) > 0) m.gacc_smem = 1;
+    }
+  }
   const bool smem_plane = meas_layout(m, true, kGreen).total <= static_cast<size_t>(limit);
   const size_t smem = meas_layout(m, smem_plane, kGreen).total;
   if (smem > static_cast<size_t>(limit)) return kErrArgument;
@@ -574,40 +712,60 @@ int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const 
 // (pairs of one-body values, one per ex entry) | TwoBodyG (ngtwo)]. Every walker's sums in
 // sample order over its valid samples are scaled by its 1/Wc, summed in walker order and
 // scaled by 1/W (normalize_physcal_green run.rs:287-316; average_physcal_rank_contributions
-// run.rs:1158-1181; accumulate_two_body_gex_sample observables.rs:110-126).
-__global__ void k_green_reduce(int W, int S, int gw, int n_one, int two_off, int ngtwo, int nex, const int* __restrict__ ex,
-                               const double* __restrict__ gval, const int* __restrict__ valid, double* __restrict__ out) {
+// run.rs:1158-1181; accumulate_two_body_gex_sample observables.rs:110-126). Pass 1: blocks
+// (x, y) sum the walkers of chunk y; pass 2 adds the chunks in order.
+__global__ void k_green_partial(int W, int S, int nchunk, int gw, int n_one, int two_off, int ngtwo, int nex,
+                                const int* __restrict__ ex, const double* __restrict__ gval,
+                                const int* __restrict__ valid, double* __restrict__ part) {
   const int width = n_one + nex + ngtwo;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= width) return;
+  const int w0 = static_cast<int>(static_cast<long long>(W) * blockIdx.y / nchunk);
+  const int w1 = static_cast<int>(static_cast<long long>(W) * (blockIdx.y + 1) / nchunk);
+  int a = -1, b = -1, col = k;
+  if (k >= n_one && k < n_one + nex) {
+    a = ex[2 * (k - n_one)];
+    b = ex[2 * (k - n_one) + 1];
+  } else if (k >= n_one + nex) {
+    col = two_off + (k - n_one - nex);
+  }
+  double tot = 0.0;
+  for (int w = w0; w < w1; ++w) {
+    double wc = 0.0, acc = 0.0;
+    for (int s = 0; s < S; ++s) {
+      const size_t smp = static_cast<size_t>(w) * S + s;
+      if (!valid[smp]) continue;
+      const double* row = gval + smp * gw;
+      wc += 1.0;
+      acc += a >= 0 ? (1.0 * row[a]) * row[b] : row[col];
+    }
+    if (wc != 0.0) acc *= 1.0 / wc;
+    tot += acc;
+  }
+  part[static_cast<size_t>(blockIdx.y) * width + k] = tot;
+}
+
+__global__ void k_green_total(int W, int nchunk, int width, const double* __restrict__ part, double* __restrict__ out) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < width; k += gridDim.x * blockDim.x) {
     double tot = 0.0;
-    for (int w = 0; w < W; ++w) {
-      double wc = 0.0, acc = 0.0;
-      for (int s = 0; s < S; ++s) {
-        const size_t smp = static_cast<size_t>(w) * S + s;
-        if (!valid[smp]) continue;
-        const double* row = gval + smp * gw;
-        wc += 1.0;
-        double v;
-        if (k < n_one) v = row[k];
-        else if (k < n_one + nex) v = (1.0 * row[ex[2 * (k - n_one)]]) * row[ex[2 * (k - n_one) + 1]];
-        else v = row[two_off + (k - n_one - nex)];
-        acc += v;
-      }
-      if (wc != 0.0) acc *= 1.0 / wc;
-      tot += acc;
-    }
+    for (int c = 0; c < nchunk; ++c) tot += part[static_cast<size_t>(c) * width + k];
     if (W > 1) tot *= 1.0 / W;
     out[k] = tot;
   }
 }
 
+int green_chunks(int W) { return std::max(1, std::min(W, 64)); }
+
 int launch_green_reduce(const DevModel& m, int W, int S, int n_one, int nex, const int* ex, const double* gval,
-                        const int* valid, double* out, cudaStream_t stream) {
+                        const int* valid, double* part, double* out, cudaStream_t stream) {
   const int width = n_one + nex + m.ngtwo;
   if (width == 0) return kOk;
+  const int nchunk = green_chunks(W);
   // the TwoBodyG values sit after all ngone one-body values of the row
-  k_green_reduce<<<(width + 127) / 128, 128, 0, stream>>>(W, S, m.gw, n_one, m.ngone, m.ngtwo, nex, ex, gval, valid,
-                                                          out);
+  k_green_partial<<<dim3((width + 127) / 128, nchunk), 128, 0, stream>>>(W, S, nchunk, m.gw, n_one, m.ngone, m.ngtwo,
+                                                                         nex, ex, gval, valid, part);
+  MVMCB_CUDA(cudaGetLastError());
+  k_green_total<<<(width + 255) / 256, 256, 0, stream>>>(W, nchunk, width, part, out);
   MVMCB_CUDA(cudaGetLastError());
   return kOk;
 }

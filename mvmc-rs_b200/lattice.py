@@ -61,8 +61,13 @@ class Lattice:
 def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1), nmp=1, shifts=None,
                  nsp_gauss_leg=1, warmup=10, interval=1, samples=10, steps=10, ex_path=1,
                  seed=12345, step_dt=0.02, red_cut=1e-8, sta_del=0.02, param_seed=2024,
-                 cg_max_iter=200, cg_tol=1e-6, cg_abort=0, nsrcg=1):
-    """Write a complete input set; returns (namelist path, initial.def path, dims)."""
+                 cg_max_iter=200, cg_tol=1e-6, cg_abort=0, nsrcg=1, calc_mode=0, green=None, data_qty=1):
+    """Write a complete input set; returns (namelist path, initial.def path, dims).
+
+    calc_mode=1 writes a PhysCal set (NVMCCalMode 1, NDataQtySmp data_qty) whose fixed
+    parameters are initial.def; green="corr" adds the correlation lists: every same-spin
+    one-body term c†_{i s} c_{j s} (2·Ns² terms) and every density-density term
+    n_{i s} n_{j t} = c†_{i s} c_{i s} c†_{j t} c_{j t} (4·Ns² terms)."""
     os.makedirs(out_dir, exist_ok=True)
     lat = Lattice(lx, ly)
     ns = lat.n
@@ -70,21 +75,31 @@ def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1),
     files = dict(ModPara="modpara.def", LocSpin="locspn.def", Trans="trans.def",
                  CoulombIntra="coulombintra.def", Gutzwiller="gutzwilleridx.def",
                  Jastrow="jastrowidx.def", Orbital="orbitalidx.def", TransSym="qptransidx.def")
+    if green == "corr":
+        files.update(OneBodyG="greenone.def", TwoBodyG="greentwo.def")
+    elif green is not None:
+        raise ValueError(f"unknown Green list {green!r}")
     with open(os.path.join(out_dir, "namelist.def"), "w") as f:
         for k, v in files.items():
             f.write(f"{k:>16s}  {v}\n")
-    mod = dict(NVMCCalMode=0, Nsite=ns, Ncond=2 * n_up, **{"2Sz": 0}, NSPGaussLeg=nsp_gauss_leg,
+    mod = dict(NVMCCalMode=calc_mode, Nsite=ns, Ncond=2 * n_up, **{"2Sz": 0}, NSPGaussLeg=nsp_gauss_leg,
                NSPStot=0, NMPTrans=nmp, NSROptItrStep=steps, NSROptItrSmp=max(1, steps // 10),
                DSROptRedCut=red_cut, DSROptStaDel=sta_del, DSROptStepDt=step_dt, NVMCWarmUp=warmup,
                NVMCInterval=interval, NVMCSample=samples, NExUpdatePath=ex_path, RndSeed=seed,
                NSplitSize=1, NStore=1, NSRCG=nsrcg, NSROptCGMaxIter=cg_max_iter, DSROptCGTol=cg_tol,
-               NSRCGAbortOnFail=cg_abort)
+               NSRCGAbortOnFail=cg_abort, NDataIdxStart=0, NDataQtySmp=data_qty)
     with open(os.path.join(out_dir, "modpara.def"), "w") as f:
         f.write("--------------------\nModel_Parameters   0\n--------------------\n"
                 "VMC_Cal_Parameters\n--------------------\nCDataFileHead  zvo\n"
                 "CParaFileHead  zqp\n--------------------\n")
         for k, v in mod.items():
             f.write(f"{k:<14s} {v}\n")
+    if green == "corr":
+        _def_file(os.path.join(out_dir, "greenone.def"), "NCisAjs", 2 * ns * ns,
+                  "".join(f"{i:5d} {s:5d} {j:5d} {s:5d}\n" for s in (0, 1) for i in range(ns) for j in range(ns)))
+        _def_file(os.path.join(out_dir, "greentwo.def"), "NCisAjsCktAltDC", 4 * ns * ns,
+                  "".join(f"{i:5d} {s:5d} {i:5d} {s:5d} {j:5d} {t:5d} {j:5d} {t:5d}\n"
+                          for i in range(ns) for j in range(ns) for s in (0, 1) for t in (0, 1)))
     _def_file(os.path.join(out_dir, "locspn.def"), "NlocalSpin", 0,
               "".join(f"{i:5d} 0\n" for i in range(ns)))
     lines = []
@@ -164,4 +179,9 @@ CONFIGS = {
     # As square16 with 4×4-sublattice f (4096).
     "square16_sr": dict(lx=16, ly=16, U=6.0, tp=-0.2, n_up=112, sub=(4, 4), nmp=1, nsp_gauss_leg=1,
                         interval=1, samples=1, warmup=4, steps=50, seed=12345),
+    # PhysCal on the square8 model: fixed parameters, energy plus the one-body and the
+    # density-density Green functions of every site pair (8192 + 16384 terms).
+    "physcal8": dict(lx=8, ly=8, U=4.0, sub=(2, 1), nmp=4, shifts=[(0, 0), (1, 0), (0, 1), (1, 1)],
+                     nsp_gauss_leg=2, interval=1, samples=1, warmup=4, steps=10, seed=12345, calc_mode=1,
+                     green="corr"),
 }

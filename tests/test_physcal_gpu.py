@@ -62,7 +62,15 @@ def test_run_physcal_writes_the_c_files(tmp_path):
                         assert x == y, (name, a, b)
 
 
-def test_all_two_body_branches_match_oracle_on_the_chain(tmp_path):
+@pytest.fixture(params=["0", "1"], ids=["per-term", "dense"])
+def one_body_path(request, monkeypatch):
+    """The one-body plane sums per term (warp per allowed hop) or as the dense product over
+    all (empty site, electron) pairs."""
+    monkeypatch.setenv("MVMC_B200_GREEN_DENSE", request.param)
+    return request.param
+
+
+def test_all_two_body_branches_match_oracle_on_the_chain(tmp_path, one_body_path):
     one, two, ex = green_term_mix(6, np.random.default_rng(3))
     nl = write_green_lists(os.path.join(D, "inputs"), str(tmp_path / "in"), one, two, ex)
     W = 3
@@ -78,7 +86,7 @@ def test_all_two_body_branches_match_oracle_on_the_chain(tmp_path):
     eng.close()
 
 
-def test_green_functions_on_square8_match_oracle(tmp_path):
+def test_green_functions_on_square8_match_oracle(tmp_path, one_body_path):
     """2D 8×8 (n = 64, 8 QP planes): the planes live in shared memory during the
     measurement; 8 chains of 4 samples each."""
     lat = lattice()
@@ -89,7 +97,7 @@ def test_green_functions_on_square8_match_oracle(tmp_path):
     rng = np.random.default_rng(9)
     ns = 64
     one = [(int(i), s, int(j), s) for s in (0, 1) for i, j in rng.integers(0, ns, (40, 2))]
-    one += [(i, 0, i, 0) for i in range(4)] + [(0, 0, 1, 1)]
+    one += [(i, 0, i, 0) for i in range(4)] + [(0, 0, 1, 1)] + [one[3], one[50]]  # repeats too
     _, two, ex = green_term_mix(ns, rng, n_two=120)
     nl = write_green_lists(os.path.dirname(nl0), str(tmp_path / "pc"), one, two, ex[:4])
     with open(os.path.join(os.path.dirname(nl), "modpara.def")) as f:
@@ -109,4 +117,22 @@ def test_green_functions_on_square8_match_oracle(tmp_path):
     assert o_close(e[1:], ref["energy"][0], 1e-10)
     assert o_close(o1, ref["one"][0], 1e-10) and o_close(ox, ref["ex"][0], 1e-10)
     assert o_close(o2, ref["two"][0], 1e-10)
+    eng.close()
+
+
+def test_correlation_lists_on_square8_match_oracle(tmp_path, one_body_path):
+    """The bench workload's lists (every same-spin one-body pair, every density-density
+    pair) on 8 chains: the dense product path by default."""
+    lat = lattice()
+    cfg = dict(lat.CONFIGS["physcal8"])
+    cfg.update(samples=2, warmup=2)
+    nl, init, dims = lat.write_inputs(str(tmp_path / "in"), **cfg)
+    W = 8
+    g, ref = ol.physcal_green(nl, init, 4, W)
+    eng = mvmc().Engine(nl, physcal_zqp=init, walkers=W, precision=64, seed=4)
+    assert eng.green_dims["one"] == 8192 and eng.green_dims["two"] == 16384
+    eng.sample()
+    e, o1, ox, o2 = eng.measure_green()
+    assert o_close(e[1:], ref["energy"][0], 1e-10)
+    assert o_close(o1, ref["one"][0], 1e-10) and o_close(o2, ref["two"][0], 1e-10)
     eng.close()

@@ -8,6 +8,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
+#include <map>
+#include <cstring>
+#include <cstdlib>
+#include <cstdio>
 #include <vector>
 
 #include "../../include/mvmc_b200.h"
@@ -124,7 +129,7 @@ int dispatch_pfinv_pp(const double* x, const int* sizes, const long long* offset
 // first barrier. Two barriers per pivot; buffers are double-buffered by step parity; the
 // swept set is a 128-bit mask kept identically by every thread.
 template <typename T, int G, int R>
-__global__ void __launch_bounds__(G * G, (G == 8 ? (sizeof(T) == 8 ? 4 : 6) : (G == 16 ? (sizeof(T) == 8 ? 3 : 4) : 1)))
+__global__ void __launch_bounds__(G * G, (G == 8 ? (sizeof(T) == 8 ? 4 : 6) : (G == 16 ? (R >= 8 ? 1 : (sizeof(T) == 8 ? 3 : 4)) : 1)))
     k_pfinv_reg(const double* __restrict__ x, const int* __restrict__ sizes,
                 const long long* __restrict__ offsets, int n_uniform, int planes, int n_max,
                 double* __restrict__ pf, double* __restrict__ inv, int* __restrict__ status) {
@@ -335,13 +340,93 @@ int launch_pfinv_reg(const double* x, const int* sizes, const long long* offsets
   return kOk;
 }
 
+// ---- tile-shape autotuner of the register sweep ----------------------------------------
+// Every candidate computes each element with the same two-FMA update, the same first-maximum
+// pivot search and the same Pf product order, so the choice changes the speed and never the
+// bits. Candidates per size class: G×G threads with R×R elements each, n ≤ G·R.
+struct RegTile {
+  int g, r;
+};
+
+template <typename T>
+int launch_reg_tile(RegTile t, const double* x, const int* sizes, const long long* offsets, int n_uniform,
+                    int planes, int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
+#define MVMCB_TILE(G, R)                                                                                   \
+  if (t.g == G && t.r == R && n_max <= G * R)                                                              \
+    return launch_pfinv_reg<T, G, R>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  MVMCB_TILE(16, 2)
+  MVMCB_TILE(8, 4)
+  MVMCB_TILE(16, 4)
+  MVMCB_TILE(8, 8)
+  MVMCB_TILE(32, 4)
+  MVMCB_TILE(16, 8)
+#undef MVMCB_TILE
+  return kErrArgument;
+}
+
+std::vector<RegTile> reg_tile_candidates(int n_max) {
+  if (n_max <= 32) return {{16, 2}, {8, 4}};
+  if (n_max <= 64) return {{16, 4}, {8, 8}};
+  return {{32, 4}, {16, 8}};
+}
+
+// MVMC_B200_PFINV_TILE=GxR forces a tile; MVMC_B200_AUTOTUNE=0 keeps the first candidate.
+// Otherwise the first call for a (precision, size class, planes bucket) times every
+// candidate on the caller's own batch (two launches each after one warm-up, CUDA events on
+// the caller's stream) and keeps the fastest for the process.
 template <typename T>
 int dispatch_pfinv_reg(const double* x, const int* sizes, const long long* offsets, int n_uniform, int planes,
                        int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
-  // (an 8×8-thread tile with 8×8 elements per thread measured 24 % slower at n = 64)
-  if (n_max <= 32) return launch_pfinv_reg<T, 16, 2>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
-  if (n_max <= 64) return launch_pfinv_reg<T, 16, 4>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
-  return launch_pfinv_reg<T, 32, 4>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  const std::vector<RegTile> cand = reg_tile_candidates(n_max);
+  if (const char* f = std::getenv("MVMC_B200_PFINV_TILE")) {
+    RegTile t{0, 0};
+    if (std::sscanf(f, "%dx%d", &t.g, &t.r) == 2)
+      return launch_reg_tile<T>(t, x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  }
+  const char* a = std::getenv("MVMC_B200_AUTOTUNE");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(stream, &cap);
+  if ((a && std::strcmp(a, "0") == 0) || cap != cudaStreamCaptureStatusNone)
+    return launch_reg_tile<T>(cand[0], x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+  static std::mutex mu;
+  static std::map<long long, int> chosen;
+  const int cls = n_max <= 32 ? 32 : (n_max <= 64 ? 64 : 128);
+  int bucket = 0;
+  while ((1 << bucket) < planes && bucket < 30) ++bucket;
+  const long long key = (static_cast<long long>(sizeof(T)) * 1000 + cls) * 64 + bucket;
+  int pick = -1;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = chosen.find(key);
+    if (it != chosen.end()) pick = it->second;
+  }
+  if (pick < 0) {
+    cudaEvent_t e0, e1;
+    MVMCB_CUDA(cudaEventCreate(&e0));
+    MVMCB_CUDA(cudaEventCreate(&e1));
+    float best = 0.0f;
+    for (size_t c = 0; c < cand.size(); ++c) {
+      int rc = launch_reg_tile<T>(cand[c], x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+      if (rc != kOk) continue;
+      MVMCB_CUDA(cudaEventRecord(e0, stream));
+      for (int rep = 0; rep < 2 && rc == kOk; ++rep)
+        rc = launch_reg_tile<T>(cand[c], x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
+      MVMCB_CUDA(cudaEventRecord(e1, stream));
+      MVMCB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      MVMCB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rc == kOk && (pick < 0 || ms < best)) {
+        best = ms;
+        pick = static_cast<int>(c);
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (pick < 0) pick = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    chosen[key] = pick;
+  }
+  return launch_reg_tile<T>(cand[pick], x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);
 }
 
 template <typename T>

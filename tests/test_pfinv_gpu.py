@@ -101,3 +101,20 @@ def test_pfinv_singular_plane_reports_status():
     pf, inv, st = m.pfinv_batch(colmajor(x), 4, 2)
     assert st[0] > 0 and pf[0] == 0.0
     assert st[1] == 0
+
+
+@pytest.mark.parametrize("n,tiles", [(32, ["16x2", "8x4"]), (64, ["16x4", "8x8"]), (96, ["32x4", "16x8"]),
+                                     (128, ["32x4", "16x8"])])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_autotuner_candidates_give_identical_bits(n, tiles, precision, monkeypatch):
+    """The tile shapes the autotuner chooses between compute every element with the same
+    operations: Pf, the inverse and the status agree bitwise with the tuned default."""
+    m = mvmc()
+    x = colmajor(skew_batch(np.random.default_rng(3 * n), n, 300))
+    base = m.pfinv_batch_mixed(x, [n] * 300, precision)
+    for t in tiles:
+        monkeypatch.setenv("MVMC_B200_PFINV_TILE", t)
+        got = m.pfinv_batch_mixed(x, [n] * 300, precision)
+        for a, b in zip(base, got):
+            assert np.array_equal(a, b), t
+    monkeypatch.setenv("MVMC_B200_PFINV_TILE", "")

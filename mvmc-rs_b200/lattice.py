@@ -61,9 +61,12 @@ class Lattice:
 def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1), nmp=1, shifts=None,
                  nsp_gauss_leg=1, warmup=10, interval=1, samples=10, steps=10, ex_path=1,
                  seed=12345, step_dt=0.02, red_cut=1e-8, sta_del=0.02, param_seed=2024,
-                 cg_max_iter=200, cg_tol=1e-6, cg_abort=0, nsrcg=1, calc_mode=0, green=None, data_qty=1):
+                 cg_max_iter=200, cg_tol=1e-6, cg_abort=0, nsrcg=1, calc_mode=0, green=None, data_qty=1,
+                 V=0.0, J_hund=0.0):
     """Write a complete input set; returns (namelist path, initial.def path, dims).
 
+    V and J_hund add nearest-neighbour CoulombInter (V n_i n_j) and Hund
+    (−J (n_i↑n_j↑ + n_i↓n_j↓)) terms on every bond.
     calc_mode=1 writes a PhysCal set (NVMCCalMode 1, NDataQtySmp data_qty) whose fixed
     parameters are initial.def; green="corr" adds the correlation lists: every same-spin
     one-body term c†_{i s} c_{j s} (2·Ns² terms) and every density-density term
@@ -75,6 +78,10 @@ def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1),
     files = dict(ModPara="modpara.def", LocSpin="locspn.def", Trans="trans.def",
                  CoulombIntra="coulombintra.def", Gutzwiller="gutzwilleridx.def",
                  Jastrow="jastrowidx.def", Orbital="orbitalidx.def", TransSym="qptransidx.def")
+    if V != 0.0:
+        files["CoulombInter"] = "coulombinter.def"
+    if J_hund != 0.0:
+        files["Hund"] = "hund.def"
     if green == "corr":
         files.update(OneBodyG="greenone.def", TwoBodyG="greentwo.def")
     elif green is not None:
@@ -108,6 +115,13 @@ def write_inputs(out_dir, lx, ly=1, t=1.0, tp=0.0, U=4.0, n_up=None, sub=(1, 1),
             for s in (0, 1):
                 lines.append(f"{i:5d} {s:5d} {j:5d} {s:5d} {amp: .15f} {0.0: .15f}\n")
     _def_file(os.path.join(out_dir, "trans.def"), "NTransfer", len(lines), "".join(lines))
+    bonds = sorted({(min(i, j), max(i, j)) for i in range(ns) for j, _ in lat.neighbours(i, t, 0.0) if i != j})
+    if V != 0.0:
+        _def_file(os.path.join(out_dir, "coulombinter.def"), "NCoulombInter", len(bonds),
+                  "".join(f"{i:5d} {j:5d} {V: .15f}\n" for i, j in bonds))
+    if J_hund != 0.0:
+        _def_file(os.path.join(out_dir, "hund.def"), "NHund", len(bonds),
+                  "".join(f"{i:5d} {j:5d} {J_hund: .15f}\n" for i, j in bonds))
     _def_file(os.path.join(out_dir, "coulombintra.def"), "NCoulombIntra", ns,
               "".join(f"{i:5d} {U: .15f}\n" for i in range(ns)))
     _def_file(os.path.join(out_dir, "gutzwilleridx.def"), "NGutzwillerIdx", 1,

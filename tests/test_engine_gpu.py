@@ -179,3 +179,29 @@ def test_full_optimisation_matches_oracle_zvo_out(tmp_path):
     sb = [l.split() for l in open(odir / "zvo_SRinfo.dat").read().splitlines()[1:]]
     assert [r[:4] for r in sa] == [r[:4] for r in sb]  # NPara, active size, cuts
     assert all(int(r[-1]) >= 0 for r in sa)  # CG converged at every step
+
+
+@pytest.mark.parametrize("ex_path", [0, 1, 2])
+def test_interaction_terms_and_update_paths_match_oracle(tmp_path, ex_path):
+    """1D L16 with CoulombInter and Hund terms beside U, under each NExUpdatePath (0: hops
+    only, 1: hops and exchanges, 2: exchanges only): four chains' configurations, counters
+    and draw counts exact, energies and operands within 1e-12 of the oracle."""
+    from mvmc_lib import lattice
+    lat = lattice()
+    nl, init, _ = lat.write_inputs(str(tmp_path / "in"), lx=16, U=4.0, V=1.5, J_hund=0.7, ex_path=ex_path,
+                                   warmup=4, samples=3, interval=2)
+    W = 4
+    dims, ref = ol.opt_step1_walkers(nl, W, seed=7, initial_def=init)
+    eng = mvmc().Engine(nl, init, walkers=W, precision=64, seed=7)
+    eng.sample()
+    got = eng.samples()
+    assert got["ele_idx"].tolist() == ref["ele_idx"].tolist()
+    assert got["counter"].tolist() == ref["counter"].tolist()
+    assert got["draws"].tolist() == ref["draws"].tolist()
+    c = got["counter"].reshape(W, 6).sum(axis=0)
+    assert (c[0] > 0) == (ex_path != 2) and (c[2] > 0) == (ex_path != 0)
+    e, ho, oo = eng.measure()
+    assert np.allclose(e, ref["energy"], rtol=1e-12, atol=1e-13)
+    assert np.allclose(ho, ref["ho"], rtol=1e-12, atol=1e-13)
+    assert np.allclose(oo, ref["oo"], rtol=1e-12, atol=1e-13)
+    eng.close()

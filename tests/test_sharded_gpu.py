@@ -17,9 +17,10 @@ pytestmark = pytest.mark.gpu
 def test_sharded_step_on_one_rank_matches_engine_sr(tmp_path):
     lat = lattice()
     cfg = dict(lat.CONFIGS["square8"])
-    # a tight CG tolerance and a larger diagonal shift: the two recurrences (different
-    # summation orders) then agree far inside the bound whatever the samples' conditioning
-    cfg.update(interval=2, cg_tol=1e-12, cg_max_iter=2000, sta_del=0.1)
+    # a tight CG tolerance (1e-10; below that the C breakdown guard |δ| < 1e-20 is reached
+    # first) and a larger diagonal shift: the two recurrences (different summation orders)
+    # then agree within 5 % of the bound over several seeds
+    cfg.update(interval=2, cg_tol=1e-10, cg_max_iter=2000, sta_del=0.1)
     nl, init, _ = lat.write_inputs(str(tmp_path / "in"), **cfg)
     # 1024 samples for 162 parameters: with 256 the SR matrix is close enough to singular
     # that the two CG recurrences (different summation orders) end up to 5e-6 apart

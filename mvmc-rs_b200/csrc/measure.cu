@@ -688,7 +688,17 @@ int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, co
                                          lpsi, valid, gval, status, stream, limit);
 }
 
+bool cluster_measure_fits(const DevModel& m, int limit);
+int launch_measure_cluster(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
+                           const int* s_cnt, int nsamples, double* scratch, size_t scratch_len, double* ostore,
+                           double* eloc, double* lpsi, int* valid, unsigned* status, int limit, cudaStream_t stream);
+
 // gval != nullptr selects the PhysCal form: Green rows [nsamples][m.gw] instead of O rows.
+// Planes that do not fit one SM's shared memory are swept by one CTA per sample in its
+// L2 workspace; MVMC_B200_MEASURE=cluster measures them with two-CTA clusters holding half
+// the rows each in shared memory (measure_cluster.cu), which measured 1.8× slower at
+// n = 224 (72.8 vs 40.2 ms for 2048 samples: two cluster barriers and two remote row reads
+// per pivot step).
 int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
                    double* eloc, double* lpsi, int* valid, double* gval, unsigned* status, cudaStream_t stream) {
@@ -696,6 +706,13 @@ int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const 
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int n = m.n;
+  if (!gval && meas_layout(m, true).total > static_cast<size_t>(limit) && cluster_measure_fits(m, limit)) {
+    const char* e = std::getenv("MVMC_B200_MEASURE");
+    if (e && std::strcmp(e, "cluster") == 0)
+      return launch_measure_cluster(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws,
+                                    static_cast<size_t>(gws_blocks) * 2 * n * n, ostore, eloc, lpsi, valid, status,
+                                    limit, stream);
+  }
 #define MVMCB_MEASURE(J) \
   launch_measure_jpl<J>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, gval, \
                         status, stream, limit)

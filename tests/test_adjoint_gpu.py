@@ -67,9 +67,12 @@ def test_o_rows_match_central_differences(tmp_path, name, over):
     eng.close()
 
 
-def test_o_rows_match_oracle_sroopt_on_32_walkers(tmp_path):
+@pytest.mark.parametrize("measure", ["single", "cluster"])
+def test_o_rows_match_oracle_sroopt_on_32_walkers(tmp_path, monkeypatch, measure):
     """2D 16x16 (t' = -0.2, 112 + 112 electrons, n = 224, inverse planes in L2): every
-    configuration of the 32 chains equals the oracle's, and so do the SROptO rows."""
+    configuration of the 32 chains equals the oracle's, and so do the SROptO rows — with
+    the measurement on one CTA per sample and on two-CTA clusters."""
+    monkeypatch.setenv("MVMC_B200_MEASURE", measure)
     nl, init, dims = inputs(tmp_path, "square16", 1)
     W = 32
     _, ref = ol.opt_step1_walkers(nl, W, seed=21, initial_def=init)

@@ -228,17 +228,25 @@ __device__ void gj_pfinv_pp(T* A, T* B, int n, double& pf_out, int& status_out) 
         const int i = i0 + r * nwarp;
         if (i >= n) continue;
         T* Di = D + static_cast<size_t>(i) * n;
+        if (i == p || i == q) {  // the pivot rows (uniform across the warp)
+#pragma unroll
+          for (int c = 0; c < JPL; ++c) {
+            const int j = lane + 32 * c;
+            if (j >= n) continue;
+            T v;
+            if (i == p) v = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
+            else v = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
+            Di[j] = v;
+          }
+          continue;
+        }
+        const T cp = -rqi[r] * ia, cq = rpi[r] * ia;  // columns p and q of this row
 #pragma unroll
         for (int c = 0; c < JPL; ++c) {
           const int j = lane + 32 * c;
           if (j >= n) continue;
-          T v;
-          if (i == p) v = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
-          else if (i == q) v = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
-          else if (j == p) v = -rqi[r] * ia;
-          else if (j == q) v = rpi[r] * ia;
-          else v = ci[r][c] + (rqi[r] * rp[c] - rpi[r] * rq[c]) * ia;
-          Di[j] = v;
+          const T v = ci[r][c] + (rqi[r] * rp[c] - rpi[r] * rq[c]) * ia;
+          Di[j] = j == p ? cp : (j == q ? cq : v);
         }
       }
     }

@@ -517,65 +517,120 @@ extern "C" int mvmc_b200_pfinv_batch_device(const double* x, const int* sizes,
 }
 
 namespace {
-struct DevBuf {
-  void* p = nullptr;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
+// Host-buffer entry points: the batch runs in chunks of about 32 MB on two streams, so the
+// copy of chunk c+1 to the device, the sweep of chunk c and the copy of chunk c−1 back
+// overlap (fully with pinned host buffers; pageable buffers are staged by the driver). The
+// device buffers and streams are kept for the process and reused by later calls.
+struct HostPipe {
+  int device = -1;
+  cudaStream_t stream[2] = {nullptr, nullptr};
+  double* x[2] = {nullptr, nullptr};
+  double* inv[2] = {nullptr, nullptr};
+  double* pf[2] = {nullptr, nullptr};
+  int* st[2] = {nullptr, nullptr};
+  int* sz[2] = {nullptr, nullptr};
+  long long* off[2] = {nullptr, nullptr};
+  size_t cap_elems = 0;
+  int cap_planes = 0;
 };
+std::mutex g_pipe_mu;
+HostPipe g_pipe;
+
+int pipe_reserve(size_t elems, int planes) {
+  int dev = 0;
+  MVMCB_CUDA(cudaGetDevice(&dev));
+  HostPipe& h = g_pipe;
+  if (h.device != dev) {
+    h = HostPipe{};  // a new device: the old buffers stay with their context
+    h.device = dev;
+    for (int b = 0; b < 2; ++b) MVMCB_CUDA(cudaStreamCreateWithFlags(&h.stream[b], cudaStreamNonBlocking));
+  }
+  if (elems > h.cap_elems || planes > h.cap_planes) {
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(h.x[b]); cudaFree(h.inv[b]); cudaFree(h.pf[b]); cudaFree(h.st[b]); cudaFree(h.sz[b]); cudaFree(h.off[b]);
+      h.x[b] = h.inv[b] = h.pf[b] = nullptr;
+      h.st[b] = h.sz[b] = nullptr;
+      h.off[b] = nullptr;
+    }
+    h.cap_elems = h.cap_planes = 0;
+    for (int b = 0; b < 2; ++b) {
+      MVMCB_CUDA(cudaMalloc(&h.x[b], elems * sizeof(double)));
+      MVMCB_CUDA(cudaMalloc(&h.inv[b], elems * sizeof(double)));
+      MVMCB_CUDA(cudaMalloc(&h.pf[b], planes * sizeof(double)));
+      MVMCB_CUDA(cudaMalloc(&h.st[b], planes * sizeof(int)));
+      MVMCB_CUDA(cudaMalloc(&h.sz[b], planes * sizeof(int)));
+      MVMCB_CUDA(cudaMalloc(&h.off[b], planes * sizeof(long long)));
+    }
+    h.cap_elems = elems;
+    h.cap_planes = planes;
+  }
+  return kOk;
+}
+
+// sizes == nullptr: uniform n_uniform planes.
+int pfinv_host(const double* x, const int* sizes, int n_uniform, int planes, int precision, double* pf, double* inv,
+               int* status) {
+  std::vector<long long> offsets(planes + 1, 0);
+  int n_max = n_uniform;
+  for (int p = 0; p < planes; ++p) {
+    const int n = sizes ? sizes[p] : n_uniform;
+    if (n <= 0 || (n & 1)) return kErrArgument;
+    offsets[p + 1] = offsets[p] + static_cast<long long>(n) * n;
+    n_max = std::max(n_max, n);
+  }
+  // chunks of about 32 MB of planes (at least one plane)
+  const long long target = (32ll << 20) / static_cast<long long>(sizeof(double));
+  std::vector<int> starts{0};
+  while (starts.back() < planes) {
+    int e = starts.back() + 1;
+    while (e < planes && offsets[e + 1] - offsets[starts.back()] <= target) ++e;
+    starts.push_back(e);
+  }
+  size_t max_elems = 0;
+  int max_planes = 0;
+  for (size_t c = 0; c + 1 < starts.size(); ++c) {
+    max_elems = std::max<size_t>(max_elems, offsets[starts[c + 1]] - offsets[starts[c]]);
+    max_planes = std::max(max_planes, starts[c + 1] - starts[c]);
+  }
+  std::lock_guard<std::mutex> lock(g_pipe_mu);
+  int rc = pipe_reserve(max_elems, max_planes);
+  if (rc != kOk) return rc;
+  HostPipe& h = g_pipe;
+  std::vector<long long> rel(max_planes);
+  for (size_t c = 0; c + 1 < starts.size(); ++c) {
+    const int b = static_cast<int>(c & 1), p0 = starts[c], np = starts[c + 1] - p0;
+    const long long e0 = offsets[p0], ne = offsets[starts[c + 1]] - e0;
+    cudaStream_t st = h.stream[b];
+    MVMCB_CUDA(cudaMemcpyAsync(h.x[b], x + e0, ne * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (sizes) {
+      for (int p = 0; p < np; ++p) rel[p] = offsets[p0 + p] - e0;
+      MVMCB_CUDA(cudaMemcpyAsync(h.sz[b], sizes + p0, np * sizeof(int), cudaMemcpyHostToDevice, st));
+      MVMCB_CUDA(cudaMemcpyAsync(h.off[b], rel.data(), np * sizeof(long long), cudaMemcpyHostToDevice, st));
+    }
+    rc = pfinv_device(h.x[b], sizes ? h.sz[b] : nullptr, sizes ? h.off[b] : nullptr, n_uniform, np, n_max, h.pf[b],
+                      h.inv[b], h.st[b], precision, st);
+    if (rc != kOk) return rc;
+    MVMCB_CUDA(cudaMemcpyAsync(inv + e0, h.inv[b], ne * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MVMCB_CUDA(cudaMemcpyAsync(pf + p0, h.pf[b], np * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MVMCB_CUDA(cudaMemcpyAsync(status + p0, h.st[b], np * sizeof(int), cudaMemcpyDeviceToHost, st));
+  }
+  for (int b = 0; b < 2; ++b) MVMCB_CUDA(cudaStreamSynchronize(h.stream[b]));
+  return kOk;
+}
 }  // namespace
 
 extern "C" int mvmc_b200_pfinv_batch(const double* x, int n, int planes, double* pf, double* inv,
                                      int* status) {
   if (n <= 0 || (n & 1) || planes < 0) return kErrArgument;
   if (planes == 0) return kOk;
-  const size_t nn = static_cast<size_t>(n) * n * planes;
-  DevBuf dx, dinv, dpf, dst;
-  MVMCB_CUDA(cudaMalloc(&dx.p, nn * sizeof(double)));
-  MVMCB_CUDA(cudaMalloc(&dinv.p, nn * sizeof(double)));
-  MVMCB_CUDA(cudaMalloc(&dpf.p, planes * sizeof(double)));
-  MVMCB_CUDA(cudaMalloc(&dst.p, planes * sizeof(int)));
-  MVMCB_CUDA(cudaMemcpy(dx.p, x, nn * sizeof(double), cudaMemcpyHostToDevice));
-  int rc = pfinv_device(static_cast<double*>(dx.p), nullptr, nullptr, n, planes, n,
-                        static_cast<double*>(dpf.p), static_cast<double*>(dinv.p),
-                        static_cast<int*>(dst.p), 64, nullptr);
-  if (rc != kOk) return rc;
-  MVMCB_CUDA(cudaMemcpy(inv, dinv.p, nn * sizeof(double), cudaMemcpyDeviceToHost));
-  MVMCB_CUDA(cudaMemcpy(pf, dpf.p, planes * sizeof(double), cudaMemcpyDeviceToHost));
-  MVMCB_CUDA(cudaMemcpy(status, dst.p, planes * sizeof(int), cudaMemcpyDeviceToHost));
-  return kOk;
+  if (!x || !pf || !inv || !status) return kErrArgument;
+  return pfinv_host(x, nullptr, n, planes, 64, pf, inv, status);
 }
 
 extern "C" int mvmc_b200_pfinv_batch_mixed(const double* x, const int* sizes, int planes,
                                            int precision, double* pf, double* inv, int* status) {
   if (planes < 0 || !sizes) return kErrArgument;
   if (planes == 0) return kOk;
-  std::vector<long long> offsets(planes);
-  long long total = 0;
-  int n_max = 0;
-  for (int p = 0; p < planes; ++p) {
-    if (sizes[p] <= 0 || (sizes[p] & 1)) return kErrArgument;
-    offsets[p] = total;
-    total += static_cast<long long>(sizes[p]) * sizes[p];
-    n_max = std::max(n_max, sizes[p]);
-  }
-  DevBuf dx, dinv, dpf, dst, dsz, doff;
-  MVMCB_CUDA(cudaMalloc(&dx.p, total * sizeof(double)));
-  MVMCB_CUDA(cudaMalloc(&dinv.p, total * sizeof(double)));
-  MVMCB_CUDA(cudaMalloc(&dpf.p, planes * sizeof(double)));
-  MVMCB_CUDA(cudaMalloc(&dst.p, planes * sizeof(int)));
-  MVMCB_CUDA(cudaMalloc(&dsz.p, planes * sizeof(int)));
-  MVMCB_CUDA(cudaMalloc(&doff.p, planes * sizeof(long long)));
-  MVMCB_CUDA(cudaMemcpy(dx.p, x, total * sizeof(double), cudaMemcpyHostToDevice));
-  MVMCB_CUDA(cudaMemcpy(dsz.p, sizes, planes * sizeof(int), cudaMemcpyHostToDevice));
-  MVMCB_CUDA(cudaMemcpy(doff.p, offsets.data(), planes * sizeof(long long), cudaMemcpyHostToDevice));
-  int rc = pfinv_device(static_cast<double*>(dx.p), static_cast<int*>(dsz.p),
-                        static_cast<long long*>(doff.p), 0, planes, n_max,
-                        static_cast<double*>(dpf.p), static_cast<double*>(dinv.p),
-                        static_cast<int*>(dst.p), precision, nullptr);
-  if (rc != kOk) return rc;
-  MVMCB_CUDA(cudaMemcpy(inv, dinv.p, total * sizeof(double), cudaMemcpyDeviceToHost));
-  MVMCB_CUDA(cudaMemcpy(pf, dpf.p, planes * sizeof(double), cudaMemcpyDeviceToHost));
-  MVMCB_CUDA(cudaMemcpy(status, dst.p, planes * sizeof(int), cudaMemcpyDeviceToHost));
-  return kOk;
+  if (!x || !pf || !inv || !status) return kErrArgument;
+  return pfinv_host(x, sizes, 0, planes, precision, pf, inv, status);
 }

@@ -38,7 +38,7 @@ constexpr int kGreenRows = 4;
 constexpr int kGreenTile = (kMeasThreads / 32) * kGreenRows;
 
 struct MeasLayout {
-  size_t idx, cfg, num, cnt, tr, sg, pf, tacc, g1, oacc, cj, gscr, gacc, gempty, gtile, gj, plane, total;
+  size_t idx, cfg, num, cnt, tr, sg, pf, tacc, g1, oacc, cj, gscr, gacc, gempty, gtile, snap, gj, plane, total;
 };
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -68,6 +68,9 @@ __host__ __device__ inline MeasLayout meas_layout(const DevModel& m, bool smem_p
   if (green && m.gdense) o = a16(o + sizeof(int) * 2 * static_cast<size_t>(m.ns));
   L.gtile = o;
   if (green && m.gdense) o = a16(o + sizeof(double) * kGreenTile * static_cast<size_t>(m.n));
+  // rows p and q of the in-place sweep of a plane in global memory
+  L.snap = o;
+  if (!smem_plane) o = a16(o + 2 * sizeof(double) * static_cast<size_t>(m.n));
   L.gj = o;
   L.plane = o;
   // the plane and its ping-pong partner
@@ -433,7 +436,11 @@ __global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
       int st;
       // planes in L2: a few rows in flight per warp, fewer for wide rows so that two
       // samples share an SM
-      gj_pfinv_pp<double, JPL, kSmemPlane ? 1 : (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, Bpp, n, pfv, st);
+      if (kSmemPlane)
+        gj_pfinv_pp<double, JPL, 1>(A, Bpp, n, pfv, st);
+      else  // in place: one plane per sample block in L2, rows p and q snapshot in shared memory
+        gj_pfinv_ip<double, JPL, (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, reinterpret_cast<double*>(smem + L.snap), n,
+                                                                       pfv, st);
       if (st != 0) {
         if (tid == 0) s_bad = 1;
         __syncthreads();

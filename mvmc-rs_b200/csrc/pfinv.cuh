@@ -148,6 +148,126 @@ __device__ void gj_pfinv(T* A, int lda, int n, const GJShared<T>& s, double& pf_
 
 namespace mvmcb {
 
+// In-place form for planes in global memory whose ping-pong partner would not stay in L2
+// beside the other resident samples: rows p and q are snapshot in shared memory (snap,
+// 2n elements) and the sweep updates A in place; three barriers per pivot step. Same
+// element arithmetic, pivot rule and status codes as gj_pfinv_pp. n <= 32·JPL, lda = n.
+template <typename T, int JPL, int RB = 1>
+__device__ void gj_pfinv_ip(T* A, T* snap, int n, double& pf_out, int& status_out) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  unsigned swept = 0;  // bit c: column lane + 32c swept
+  int p = 0, parity = 0, status = 0;
+  double pf = 1.0;
+  T* rowp = snap;
+  T* rowq = snap + n;
+  for (int k = 0; k < n / 2; ++k) {
+    for (int j = tid; j < n; j += nt) rowp[j] = A[static_cast<size_t>(p) * n + j];
+    __syncthreads();
+    T rp[JPL];
+    double best = -1.0;
+    int bi = n;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      rp[c] = j < n ? rowp[j] : T(0);
+      if (j < n && j != p && !((swept >> c) & 1u)) {
+        const double v = fabs(static_cast<double>(rp[c]));
+        if (v > best) {
+          best = v;
+          bi = j;
+        }
+      }
+    }
+    warp_argmax_first(best, bi);
+    const int q = __shfl_sync(0xffffffffu, bi, 0);
+    best = __shfl_sync(0xffffffffu, best, 0);
+    if (!(best > 0.0)) {
+      status = p + 1;
+      break;  // every warp reads the same snapshot: all leave together
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      cnt += (j < n && !((swept >> c) & 1u) && j > p && j < q) ? 1 : 0;
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    parity += cnt;
+    const T a = rowp[q];
+    pf *= static_cast<double>(a);
+    const T ia = T(1) / a;
+    for (int j = tid; j < n; j += nt) rowq[j] = A[static_cast<size_t>(q) * n + j];
+    __syncthreads();
+    T rq[JPL];
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      rq[c] = j < n ? rowq[j] : T(0);
+    }
+    for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
+      T ci[RB][JPL];
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        const T* Ci = A + static_cast<size_t>(i) * n;
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          ci[r][c] = (i < n && j < n) ? Ci[j] : T(0);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        if (i >= n) continue;
+        T* Ci = A + static_cast<size_t>(i) * n;
+        if (i == p || i == q) {
+#pragma unroll
+          for (int c = 0; c < JPL; ++c) {
+            const int j = lane + 32 * c;
+            if (j >= n) continue;
+            T v;
+            if (i == p) v = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
+            else v = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
+            Ci[j] = v;
+          }
+          continue;
+        }
+        const T rpi = rowp[i], rqi = rowq[i];
+        const T cp = -rqi * ia, cq = rpi * ia;
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j >= n) continue;
+          const T v = ci[r][c] + (rqi * rp[c] - rpi * rq[c]) * ia;
+          Ci[j] = j == p ? cp : (j == q ? cq : v);
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j == p || j == q) swept |= 1u << c;
+    }
+    int nxt = n;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j < n && !((swept >> c) & 1u) && j < nxt) nxt = j;
+    }
+    for (int off = 16; off > 0; off >>= 1) nxt = min(nxt, __shfl_xor_sync(0xffffffffu, nxt, off));
+    p = nxt < n ? nxt : 0;
+    __syncthreads();  // the swept rows are complete before the next snapshot
+  }
+  double v = (parity & 1) ? -pf : pf;
+  if (status == 0 && !isfinite(v)) status = -1;
+  if (status != 0) v = 0.0;
+  pf_out = v;
+  status_out = status;
+  __syncthreads();
+}
+
 // Ping-pong form of the sweep: one barrier per pivot step. Every warp picks the pivot
 // redundantly from the unmodified source buffer (identical data, identical choice), reads
 // rows p and q from it, and writes the swept matrix into the other buffer. Lane l owns

@@ -172,7 +172,8 @@ __device__ void update_proj_cnt_warp(const DevModel& m, const int* jtab, int ri,
 // in FP64 in ws/ws2 and rounded into the plane (the FP64 refresh of the mixed path).
 // FP64 refresh of every plane (CalculateMAll). The sweep runs in the FP64 buffers: in
 // shared memory when they are there (the plane is gathered into the first buffer and the
-// result copied to the plane), else in place on an FP64 plane in L2 with a global scratch.
+// result copied to the plane), else in place on an FP64 plane in L2 (rows p, q of each
+// pivot step snapshot in the shared GJ rows).
 template <typename T, int JPL, bool kSmemPlanes, bool kSmemWs>
 __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status) {
   const int n = m.n;
@@ -194,7 +195,12 @@ __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigne
     __syncthreads();
     double pfv;
     int st;
-    gj_pfinv_pp<double, JPL, RB>(A, B, n, pfv, st);
+    if constexpr (kInPlace && !kSmemPlanes)
+      // FP64 plane in L2: swept in place (rows p, q in shared memory), so the resident
+      // walkers' refreshes touch their own planes only
+      gj_pfinv_ip<double, JPL, RB>(A, s.gj.rowp, n, pfv, st);
+    else
+      gj_pfinv_pp<double, JPL, RB>(A, B, n, pfv, st);
     if (!kInPlace) {
       for (int k = threadIdx.x; k < n * n; k += blockDim.x) P[k] = static_cast<T>(A[k]);
     }

@@ -1004,17 +1004,21 @@ int walkers_per_sm();
 template <typename T, int JPL, int NT, bool kSmemPlanes, bool kSmemWs>
 int launch_sample_t(const DevModel& m, const DevWalkers& w, cudaStream_t stream) {
   size_t smem = samp_layout<T>(m, kSmemPlanes, kSmemWs).total;
+  auto kernel = k_sample<T, JPL, NT, kSmemPlanes, kSmemWs>;
   if (!kSmemPlanes && walkers_per_sm() > 0) {
     // cap the walkers resident per SM (so that their L2 slices stay in L2) by the
-    // shared-memory footprint of each CTA
-    int dev = 0, per_sm = 0, reserved = 0;
+    // shared-memory footprint of each CTA, within the per-block limit
+    int dev = 0, per_sm = 0, reserved = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-    const size_t cap = static_cast<size_t>(per_sm / walkers_per_sm() - reserved);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    MVMCB_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    const size_t cap = std::min(static_cast<size_t>(per_sm / walkers_per_sm() - reserved) - fa.sharedSizeBytes,
+                                static_cast<size_t>(optin) - fa.sharedSizeBytes);
     smem = std::max(smem, cap);
   }
-  auto kernel = k_sample<T, JPL, NT, kSmemPlanes, kSmemWs>;
   MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   kernel<<<w.W, NT, smem, stream>>>(m, w);
   MVMCB_CUDA(cudaGetLastError());

@@ -340,8 +340,8 @@ __device__ void green_finish(const DevModel& m, double ip, bool ok, const int* c
   __syncthreads();
 }
 
-template <int JPL, bool kSmemPlane, bool kGreen>
-__global__ void __launch_bounds__(kMeasThreads, (kSmemPlane ? 1 : 2))
+template <int JPL, bool kSmemPlane, bool kGreen, int NT = kMeasThreads>
+__global__ void __launch_bounds__(NT, (kSmemPlane || NT > kMeasThreads ? 1 : 2))
     k_measure(DevModel m, const int* __restrict__ s_idx, const int* __restrict__ s_cfg,
               const int* __restrict__ s_num, const int* __restrict__ s_cnt, int nsamples,
               double* __restrict__ gws, double* __restrict__ ostore, double* __restrict__ eloc,
@@ -668,17 +668,32 @@ int launch_measure_kind(const DevModel& m_in, const int* s_idx, const int* s_cfg
     kernel<<<nsamples, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
                                                      valid, gval, status);
   } else {
-    auto kernel = k_measure<JPL, false, kGreen>;
-    MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     // As many blocks as are co-resident, striding over the samples: each block reuses its
-    // own ping-pong workspace, so the workspaces stay in L2 across samples.
-    int dev = 0, sms = 0, per = 0;
+    // own workspace, so the workspaces stay in L2 across samples. When two 256-thread
+    // blocks per SM would hold more plane bytes than ~3/4 of the L2 (2D 16×16: 401 KB per
+    // sample), one 512-thread block per SM sweeps instead.
+    int dev = 0, sms = 0, per = 0, l2 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kMeasThreads, smem));
-    const int grid = std::max(1, std::min({nsamples, gws_blocks, sms * std::max(1, per)}));
-    kernel<<<grid, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
-                                                 valid, gval, status);
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+    const double plane_bytes = 8.0 * m.n * m.n;
+    bool wide = !kGreen && 2.0 * sms * plane_bytes > 0.75 * l2;
+    if (const char* e = std::getenv("MVMC_B200_MEAS_THREADS")) wide = !kGreen && std::strcmp(e, "512") == 0;
+    if (wide) {
+      auto kernel = k_measure<JPL, false, kGreen, 512>;
+      MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 512, smem));
+      const int grid = std::max(1, std::min({nsamples, gws_blocks, sms * std::max(1, per)}));
+      kernel<<<grid, 512, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi, valid,
+                                          gval, status);
+    } else {
+      auto kernel = k_measure<JPL, false, kGreen>;
+      MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kMeasThreads, smem));
+      const int grid = std::max(1, std::min({nsamples, gws_blocks, sms * std::max(1, per)}));
+      kernel<<<grid, kMeasThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, ostore, eloc, lpsi,
+                                                   valid, gval, status);
+    }
   }
   MVMCB_CUDA(cudaGetLastError());
   return kOk;

@@ -1115,8 +1115,19 @@ int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int
       return launch_sample_t<float, JPL, 512, true, false>(m, w, stream);
     return launch_sample_global<float, JPL>(m, w, stream);
   }
-  if (samp_layout<double>(m, true, true).total <= static_cast<size_t>(limit))
+  if (samp_layout<double>(m, true, true).total <= static_cast<size_t>(limit)) {
+    if constexpr (JPL == 1) {
+      // small planes (n ≤ 32): 128 threads per walker (1D L16: 1.95M vs 1.33M sweeps/s
+      // with 512, whose barriers cost more than the work they split); MVMC_B200_SMEM_THREADS
+      // = 64|128|256|512 overrides
+      const char* e = std::getenv("MVMC_B200_SMEM_THREADS");
+      const int nt = e ? std::atoi(e) : 128;
+      if (nt == 64) return launch_sample_t<double, JPL, 64, true, true>(m, w, stream);
+      if (nt == 128) return launch_sample_t<double, JPL, 128, true, true>(m, w, stream);
+      if (nt == 256) return launch_sample_t<double, JPL, 256, true, true>(m, w, stream);
+    }
     return launch_sample_t<double, JPL, 512, true, true>(m, w, stream);
+  }
   return launch_sample_global<double, JPL>(m, w, stream);
 }
 

@@ -1109,8 +1109,14 @@ int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int
     return launch_sample_global<double, JPL>(m, w, stream);
   }
   if (precision == 32) {
-    if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit))
+    if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit)) {
+      if constexpr (JPL == 1) {
+        // small planes: 128 threads per walker, as for FP64 below
+        const char* e = std::getenv("MVMC_B200_SMEM_THREADS");
+        if (!e || std::atoi(e) == 128) return launch_sample_t<float, JPL, 128, true, true>(m, w, stream);
+      }
       return launch_sample_t<float, JPL, 512, true, true>(m, w, stream);
+    }
     if (samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit))
       return launch_sample_t<float, JPL, 512, true, false>(m, w, stream);
     return launch_sample_global<float, JPL>(m, w, stream);

@@ -50,6 +50,13 @@ int mvmc_b200_pfinv_batch_device(const double* x, const int* sizes, const long l
                                  int n_uniform, int planes, int n_max, double* pf, double* inv,
                                  int* status, int precision, void* stream);
 
+/* Complex skew planes (the Pfaffian + inverse of the complex mode's CalculateMAll,
+ * calc_m_all_complex, crates/mvmc-core/src/pfaffian.rs:340-360): x holds `planes`
+ * column-major n×n planes of (re, im) pairs; pf receives (re, im) per plane, inv the true
+ * X⁻¹ in the same layout, status as mvmc_b200_pfinv_batch. FP64. */
+int mvmc_b200_pfinv_batch_complex(const double* x, int n, int planes, double* pf, double* inv,
+                                  int* status);
+
 /* ---------------------------------------------------------------------------------
  * Walker ensemble engine.
  * ------------------------------------------------------------------------------- */

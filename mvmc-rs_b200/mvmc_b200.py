@@ -27,7 +27,7 @@ EXPORTS = [
     "mvmc_b200_stage_state", "mvmc_b200_gram", "mvmc_b200_cholesky_solve",
     "mvmc_b200_measure_sums", "mvmc_b200_sr_gather", "mvmc_b200_sr_local_product", "mvmc_b200_sr_apply",
     "mvmc_b200_sr_config", "mvmc_b200_physcal_create", "mvmc_b200_green_dims", "mvmc_b200_measure_green",
-    "mvmc_b200_run_physcal",
+    "mvmc_b200_run_physcal", "mvmc_b200_pfinv_batch_complex",
 ]
 
 
@@ -67,6 +67,17 @@ def pfinv_batch(x_colmajor, n, planes):
     inv = np.zeros(planes * n * n)
     st = np.zeros(planes, dtype=np.int32)
     _check(lib().mvmc_b200_pfinv_batch(_ptr(x), n, planes, _ptr(pf), _ptr(inv), _ptr(st)), "pfinv_batch")
+    return pf, inv, st
+
+
+def pfinv_batch_complex(x_colmajor, n, planes):
+    """Complex skew planes (column-major, complex128): Pf (complex) and the true X⁻¹."""
+    x = np.ascontiguousarray(x_colmajor, dtype=np.complex128)
+    pf = np.zeros(planes, dtype=np.complex128)
+    inv = np.zeros(x.size, dtype=np.complex128)
+    st = np.zeros(planes, dtype=np.int32)
+    _check(lib().mvmc_b200_pfinv_batch_complex(_ptr(x), n, planes, _ptr(pf), _ptr(inv), _ptr(st)),
+           "pfinv_batch_complex")
     return pf, inv, st
 
 

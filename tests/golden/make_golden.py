@@ -75,6 +75,11 @@ def main(ref):
               names={f for f in os.listdir(src) if f.startswith("real_n") and
                      int(f.split("_")[1][1:]) <= 64})
 
+    # Complex skew test matrices (identities of the complex Pfaffian + inverse).
+    copy_tree(src, os.path.join(HERE, "pfapack_complex"),
+              names={f for f in os.listdir(src) if f.startswith("complex_n") and
+                     int(f.split("_")[1][1:]) <= 128})
+
     # C StochasticOptCG iterates on fixed operands (tol 0, shift 1e-5).
     copy_tree(os.path.join(fx, "sr_cg/c_refresh"), os.path.join(HERE, "sr_cg"),
               names={"real.txt", "real_diag_scale.txt"})

@@ -57,6 +57,12 @@ int mvmc_b200_pfinv_batch_device(const double* x, const int* sizes, const long l
 int mvmc_b200_pfinv_batch_complex(const double* x, int n, int planes, double* pf, double* inv,
                                   int* status);
 
+/* Device-buffer form of mvmc_b200_pfinv_batch_complex (PfaffianStages' complex batch on
+ * device-resident planes; stage_backend.rs:121-165): same layouts, no allocation, launched
+ * on `stream` (a cudaStream_t; NULL = default) and not synchronised. */
+int mvmc_b200_pfinv_batch_complex_device(const double* x, int n, int planes, double* pf, double* inv,
+                                         int* status, void* stream);
+
 /* ---------------------------------------------------------------------------------
  * Walker ensemble engine.
  * ------------------------------------------------------------------------------- */
@@ -73,6 +79,10 @@ typedef struct mvmc_b200_options {
                          * centred and column-scaled, FP32 products (the mixed path's operator) */
   double refresh_guard; /* g in [0, 1): FP64 refresh right after an accepted move whose Pfaffian
                          * ratio on any QP plane lies outside [g, 1/g]; 0 = off (C behaviour) */
+  int c_order;          /* 1: measurement, its sums and SR-CG in the reference CPU path's operation
+                         * order without FMA (pfapack LTLᵀ inverse, serial sums; results equal the
+                         * CPU path's bit for bit up to libm's exp): the parity mode of the 10-step
+                         * zvo_out.dat gate (phase5_zvo_gate_hubbard.rs:19-80). 0: throughput kernels. */
 } mvmc_b200_options;
 
 void mvmc_b200_default_options(mvmc_b200_options* opt);

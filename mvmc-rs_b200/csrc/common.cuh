@@ -38,6 +38,28 @@ enum DeviceStatus : unsigned {
     }                                                                            \
   } while (0)
 
+// A device attribute of the CURRENT device, cached per device ordinal (launch shapes
+// queried on one GPU must not be reused on another with fewer SMs or less shared memory).
+inline int current_device_attr(cudaDeviceAttr attr) {
+  constexpr int kMaxDevices = 64;
+  static int cache[kMaxDevices][3];  // value + 1; 0 = not queried yet
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int slot = attr == cudaDevAttrMultiProcessorCount ? 0
+                   : attr == cudaDevAttrMaxSharedMemoryPerBlockOptin ? 1
+                   : attr == cudaDevAttrL2CacheSize ? 2 : -1;
+  int value = 0;
+  if (dev < 0 || dev >= kMaxDevices || slot < 0) {
+    cudaDeviceGetAttribute(&value, attr, dev);
+    return value;
+  }
+  if (cache[dev][slot] == 0) {
+    cudaDeviceGetAttribute(&value, attr, dev);
+    cache[dev][slot] = value + 1;
+  }
+  return cache[dev][slot] - 1;
+}
+
 template <typename T>
 __device__ __forceinline__ T dev_abs(T x) {
   return x < T(0) ? -x : x;

@@ -29,6 +29,12 @@ int launch_green_reduce(const DevModel& m, int W, int S, int n_one, int nex, con
 int green_chunks(int W);
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,
                   const int* valid, const int* s_num, double* wsum, double* tot, cudaStream_t stream);
+int launch_reduce_totals(const DevModel& m, int W, const double* wsum, double* tot, cudaStream_t stream);
+void corder_scratch_sizes(const DevModel& m, long long* dstride, long long* istride);
+int launch_measure_corder(const DevModel& m, int W, int S, const int* s_idx, const int* s_cfg, const int* s_num,
+                          const int* s_cnt, double* ostore, double* eloc, double* lpsi, int* valid, double* wsum,
+                          double* dscr, int* iscr, cudaStream_t stream);
+int launch_cg_corder(const CgArgs& a, int W, int S, cudaStream_t stream);
 int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
                          double* oa, cudaStream_t stream);
 int launch_sr_cg(CgArgs a, cudaStream_t stream);
@@ -71,12 +77,14 @@ __global__ void k_slater_table(int ns, int nqp, int nleg, int nmp, const double*
     float* p32 = out32 + static_cast<size_t>(qp) * ns2 * ns2;
     double v00 = 0, v01 = 0, v10 = 0, v11 = 0;
     if (iij >= 0 && iji >= 0) {
-      const double sij = f[iij] * static_cast<double>(orb_sgn[tri * ns + trj] * qpsgn);
-      const double sji = f[iji] * static_cast<double>(orb_sgn[trj * ns + tri] * qpsgn);
-      v00 = -(sij - sji) * cs;
-      v01 = sij * cc + sji * ss;
-      v10 = -sij * ss - sji * cc;
-      v11 = (sij - sji) * cs;
+      // separately rounded products and sums (no FMA): the table equals the host's
+      // build_slater_table bit for bit
+      const double sij = __dmul_rn(f[iij], static_cast<double>(orb_sgn[tri * ns + trj] * qpsgn));
+      const double sji = __dmul_rn(f[iji], static_cast<double>(orb_sgn[trj * ns + tri] * qpsgn));
+      v00 = __dmul_rn(-__dsub_rn(sij, sji), cs);
+      v01 = __dadd_rn(__dmul_rn(sij, cc), __dmul_rn(sji, ss));
+      v10 = __dsub_rn(__dmul_rn(-sij, ss), __dmul_rn(sji, cc));
+      v11 = __dmul_rn(__dsub_rn(sij, sji), cs);
     }
     p[ri * ns2 + rj] = v00;
     p[ri * ns2 + rj + ns] = v01;
@@ -114,6 +122,8 @@ struct mvmc_b200_ctx {
   double* d_wsum = nullptr;
   double* d_tot = nullptr;
   double* d_gws = nullptr;
+  double* d_cscr = nullptr;  // C-order measurement scratch (per walker), allocated on first use
+  int* d_cscr_i = nullptr;
   int gws_blocks = 0;
   // SR-CG buffers
   double* d_oa = nullptr;
@@ -485,12 +495,26 @@ int guarded(F&& f) {
 
 int do_measure(mvmc_b200_ctx* c) {
   const int rows = c->W * c->S;
-  int rc = launch_measure(c->dm, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, rows, c->d_gws,
-                          c->gws_blocks, c->d_ostore, c->d_eloc, c->d_lpsi, c->d_valid, nullptr, c->dw.status,
-                          c->stream);
-  if (rc != kOk) return rc;
-  rc = launch_reduce(c->dm, c->W, c->S, c->d_ostore, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
-                     c->stream);
+  int rc;
+  if (c->opt.c_order) {
+    // parity mode: one thread per walker in the CPU path's operation order (csrc/corder.cu)
+    if (!c->d_cscr) {
+      long long ds = 0, is = 0;
+      corder_scratch_sizes(c->dm, &ds, &is);
+      c->d_cscr = c->alloc<double>(static_cast<size_t>(c->W) * ds);
+      c->d_cscr_i = c->alloc<int>(static_cast<size_t>(c->W) * is);
+    }
+    rc = launch_measure_corder(c->dm, c->W, c->S, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, c->d_ostore,
+                               c->d_eloc, c->d_lpsi, c->d_valid, c->d_wsum, c->d_cscr, c->d_cscr_i, c->stream);
+    if (rc != kOk) return rc;
+    rc = launch_reduce_totals(c->dm, c->W, c->d_wsum, c->d_tot, c->stream);
+  } else {
+    rc = launch_measure(c->dm, c->dw.s_idx, c->dw.s_cfg, c->dw.s_num, c->dw.s_cnt, rows, c->d_gws, c->gws_blocks,
+                        c->d_ostore, c->d_eloc, c->d_lpsi, c->d_valid, nullptr, c->dw.status, c->stream);
+    if (rc != kOk) return rc;
+    rc = launch_reduce(c->dm, c->W, c->S, c->d_ostore, c->d_eloc, c->d_valid, c->dw.s_num, c->d_wsum, c->d_tot,
+                       c->stream);
+  }
   if (rc != kOk) return rc;
   c->tot.assign(5 + 3 * c->dm.sr_size, 0.0);
   check(cudaMemcpyAsync(c->tot.data(), c->d_tot, sizeof(double) * c->tot.size(), cudaMemcpyDeviceToHost, c->stream),
@@ -686,7 +710,7 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   }
   const long long ns = static_cast<long long>(c->W) * c->S;
   // operator storage: 0 FP64 (C order), 1 FP32, 2 BF16 (centred, column-scaled)
-  const int kind = c->opt.sr_precision == 32 ? 1 : (c->opt.sr_precision == 16 ? 2 : 0);
+  const int kind = c->opt.c_order ? 0 : (c->opt.sr_precision == 32 ? 1 : (c->opt.sr_precision == 16 ? 2 : 0));
   const size_t oa_need = kind == 0 ? static_cast<size_t>(ns) * na
                                    : (static_cast<size_t>(ns) * low_lda(na, kind) * (kind == 1 ? 4 : 2) + 7) / 8;
   if (oa_need > c->oa_cap) {
@@ -756,7 +780,8 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
     a.lda = low_lda(na, kind);
     a.o_kind = kind;
   }
-  rc = launch_sr_cg(a, c->stream);
+  auto solve = [&]() { return c->opt.c_order ? launch_cg_corder(a, c->W, c->S, c->stream) : launch_sr_cg(a, c->stream); };
+  rc = solve();
   if (rc != kOk) return rc;
   std::vector<double> x(na), scal(8);
   check(cudaMemcpyAsync(x.data(), a.x, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
@@ -770,7 +795,7 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
     const long long fallback_iter = std::max(-status - 1, 0LL);
     if (m.cg_fallback) {
       a.diag_scale = !a.diag_scale;
-      rc = launch_sr_cg(a, c->stream);
+      rc = solve();
       if (rc != kOk) return rc;
       check(cudaMemcpyAsync(x.data(), a.x, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
       check(cudaMemcpyAsync(scal.data(), c->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->stream), "download");

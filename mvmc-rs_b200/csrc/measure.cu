@@ -809,6 +809,16 @@ int launch_green_reduce(const DevModel& m, int W, int S, int n_one, int nex, con
   return kOk;
 }
 
+// Walker-order totals and weight average of per-walker sums already in wsum.
+int launch_reduce_totals(const DevModel& m, int W, const double* wsum, double* tot, cudaStream_t stream) {
+  const int width = 5 + 3 * m.sr_size;
+  k_reduce_total<<<(width + 255) / 256, 256, 0, stream>>>(W, m.sr_size, wsum, tot);
+  MVMCB_CUDA(cudaGetLastError());
+  k_weight_average<<<(width + 255) / 256, 256, 0, stream>>>(m.sr_size, tot);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
 int launch_reduce(const DevModel& m, int W, int S, const double* ostore, const double* eloc,
                   const int* valid, const int* s_num, double* wsum, double* tot, cudaStream_t stream) {
   k_reduce_walker<<<W, 256, 0, stream>>>(m, ostore, eloc, valid, s_num, S, wsum);

@@ -23,6 +23,8 @@ namespace mvmcb {
 
 constexpr int kPfinvThreads = 256;
 int device_sm_count();
+int pfinv_complex_device(const double* x, int n, int planes, double* pf, double* inv, int* status,
+                         cudaStream_t stream);
 
 // Column-major X read row-major is Xᵀ = −X, so loading −buffer gives X row-major and the
 // row-major X⁻¹ negated is the column-major X⁻¹.
@@ -436,25 +438,9 @@ size_t pfinv_smem_bytes(int n_max, bool smem_matrix) {
   return b;
 }
 
-int device_smem_limit() {
-  static int limit = -1;
-  if (limit < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  }
-  return limit;
-}
+int device_smem_limit() { return current_device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin); }
 
-int device_sm_count() {
-  static int count = -1;
-  if (count < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
-  }
-  return count;
-}
+int device_sm_count() { return current_device_attr(cudaDevAttrMultiProcessorCount); }
 
 template <typename T, bool kSmem>
 int launch_pfinv(const double* x, const int* sizes, const long long* offsets, int n_uniform,
@@ -567,9 +553,20 @@ int pipe_reserve(size_t elems, int planes) {
   return kOk;
 }
 
-// sizes == nullptr: uniform n_uniform planes.
-int pfinv_host(const double* x, const int* sizes, int n_uniform, int planes, int precision, double* pf, double* inv,
-               int* status) {
+// Drains both pipe streams when a call leaves early, so that no copy into the caller's
+// host buffers is still in flight when the caller regains them.
+struct PipeDrain {
+  HostPipe& h;
+  ~PipeDrain() {
+    for (int b = 0; b < 2; ++b)
+      if (h.stream[b]) cudaStreamSynchronize(h.stream[b]);
+  }
+};
+
+// sizes == nullptr: uniform n_uniform planes. comps = 1 for real planes, 2 for complex
+// planes ((re, im) pairs; uniform sizes only).
+int pfinv_host(const double* x, const int* sizes, int n_uniform, int planes, int precision, int comps, double* pf,
+               double* inv, int* status) {
   std::vector<long long> offsets(planes + 1, 0);
   int n_max = n_uniform;
   for (int p = 0; p < planes; ++p) {
@@ -579,7 +576,7 @@ int pfinv_host(const double* x, const int* sizes, int n_uniform, int planes, int
     n_max = std::max(n_max, n);
   }
   // chunks of about 32 MB of planes (at least one plane)
-  const long long target = (32ll << 20) / static_cast<long long>(sizeof(double));
+  const long long target = (32ll << 20) / static_cast<long long>(sizeof(double) * comps);
   std::vector<int> starts{0};
   while (starts.back() < planes) {
     int e = starts.back() + 1;
@@ -593,25 +590,30 @@ int pfinv_host(const double* x, const int* sizes, int n_uniform, int planes, int
     max_planes = std::max(max_planes, starts[c + 1] - starts[c]);
   }
   std::lock_guard<std::mutex> lock(g_pipe_mu);
-  int rc = pipe_reserve(max_elems, max_planes);
+  int rc = pipe_reserve(max_elems * comps, max_planes * comps);
   if (rc != kOk) return rc;
   HostPipe& h = g_pipe;
+  PipeDrain drain{h};
   std::vector<long long> rel(max_planes);
   for (size_t c = 0; c + 1 < starts.size(); ++c) {
     const int b = static_cast<int>(c & 1), p0 = starts[c], np = starts[c + 1] - p0;
-    const long long e0 = offsets[p0], ne = offsets[starts[c + 1]] - e0;
+    const long long e0 = offsets[p0] * comps, ne = (offsets[starts[c + 1]] - offsets[p0]) * comps;
     cudaStream_t st = h.stream[b];
     MVMCB_CUDA(cudaMemcpyAsync(h.x[b], x + e0, ne * sizeof(double), cudaMemcpyHostToDevice, st));
     if (sizes) {
-      for (int p = 0; p < np; ++p) rel[p] = offsets[p0 + p] - e0;
+      for (int p = 0; p < np; ++p) rel[p] = offsets[p0 + p] - offsets[p0];
       MVMCB_CUDA(cudaMemcpyAsync(h.sz[b], sizes + p0, np * sizeof(int), cudaMemcpyHostToDevice, st));
       MVMCB_CUDA(cudaMemcpyAsync(h.off[b], rel.data(), np * sizeof(long long), cudaMemcpyHostToDevice, st));
     }
-    rc = pfinv_device(h.x[b], sizes ? h.sz[b] : nullptr, sizes ? h.off[b] : nullptr, n_uniform, np, n_max, h.pf[b],
-                      h.inv[b], h.st[b], precision, st);
+    if (comps == 2)
+      rc = pfinv_complex_device(h.x[b], n_uniform, np, h.pf[b], h.inv[b], h.st[b], st);
+    else
+      rc = pfinv_device(h.x[b], sizes ? h.sz[b] : nullptr, sizes ? h.off[b] : nullptr, n_uniform, np, n_max,
+                        h.pf[b], h.inv[b], h.st[b], precision, st);
     if (rc != kOk) return rc;
     MVMCB_CUDA(cudaMemcpyAsync(inv + e0, h.inv[b], ne * sizeof(double), cudaMemcpyDeviceToHost, st));
-    MVMCB_CUDA(cudaMemcpyAsync(pf + p0, h.pf[b], np * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MVMCB_CUDA(cudaMemcpyAsync(pf + static_cast<size_t>(p0) * comps, h.pf[b], np * comps * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
     MVMCB_CUDA(cudaMemcpyAsync(status + p0, h.st[b], np * sizeof(int), cudaMemcpyDeviceToHost, st));
   }
   for (int b = 0; b < 2; ++b) MVMCB_CUDA(cudaStreamSynchronize(h.stream[b]));
@@ -624,7 +626,7 @@ extern "C" int mvmc_b200_pfinv_batch(const double* x, int n, int planes, double*
   if (n <= 0 || (n & 1) || planes < 0) return kErrArgument;
   if (planes == 0) return kOk;
   if (!x || !pf || !inv || !status) return kErrArgument;
-  return pfinv_host(x, nullptr, n, planes, 64, pf, inv, status);
+  return pfinv_host(x, nullptr, n, planes, 64, 1, pf, inv, status);
 }
 
 extern "C" int mvmc_b200_pfinv_batch_mixed(const double* x, const int* sizes, int planes,
@@ -632,5 +634,13 @@ extern "C" int mvmc_b200_pfinv_batch_mixed(const double* x, const int* sizes, in
   if (planes < 0 || !sizes) return kErrArgument;
   if (planes == 0) return kOk;
   if (!x || !pf || !inv || !status) return kErrArgument;
-  return pfinv_host(x, sizes, 0, planes, precision, pf, inv, status);
+  return pfinv_host(x, sizes, 0, planes, precision, 1, pf, inv, status);
+}
+
+extern "C" int mvmc_b200_pfinv_batch_complex(const double* x, int n, int planes, double* pf, double* inv,
+                                             int* status) {
+  if (n <= 0 || (n & 1) || planes < 0) return kErrArgument;
+  if (planes == 0) return kOk;
+  if (!x || !pf || !inv || !status) return kErrArgument;
+  return pfinv_host(x, nullptr, n, planes, 64, 2, pf, inv, status);
 }

@@ -3,8 +3,10 @@
 // 340-360, which runs pfapack's complex LTLᵀ per QP plane).
 //
 // Same skew Gauss–Jordan sweep with 2×2 pivots as the real kernels (pfinv.cuh), in complex
-// FP64: p = smallest unswept index, q = the first maximum of |A[p][j]|² over unswept j ≠ p,
-// A[i][j] += (A[q][i]·A[p][j] − A[p][i]·A[q][j]) / a with a = A[p][q], Pf = sgn(σ)·Πa.
+// FP64: p = smallest unswept index, q = the first maximum of |Re A[p][j]| + |Im A[p][j]|
+// over unswept j ≠ p (the 1-norm of IZAMAX that zsktf2 pivots by, crates/pfapack/src/ltl.rs:
+// 38-41, which neither underflows nor overflows where |z|² would),
+// A[i][j] += (A[q][i]/a)·A[p][j] − (A[p][i]/a)·A[q][j] with a = A[p][q], Pf = sgn(σ)·Πa.
 // One CTA per plane sweeps it in place in the output buffer (L2-resident), rows p and q
 // snapshot in shared memory. Planes are column-major (re, im) pairs as the real entry point
 // takes them; the returned inverse is the true X⁻¹.
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(kCplxThreads)
         int bi = n;
         for (int j = lane; j < n; j += 32) {
           if (!swept[j] && j != p) {
-            const double v = rowp[j].re * rowp[j].re + rowp[j].im * rowp[j].im;
+            const double v = fabs(rowp[j].re) + fabs(rowp[j].im);
             if (v > best) {
               best = v;
               bi = j;
@@ -110,12 +112,14 @@ __global__ void __launch_bounds__(kCplxThreads)
           for (int j = lane; j < n; j += 32)
             Ai[j] = (j == p) ? ia : (j == q ? cplx{0.0, 0.0} : cneg(cmul(rowp[j], ia)));
         } else {
-          const cplx rpi = rowp[i], rqi = rowq[i];
+          // coefficients scaled by 1/a first (as LTLᵀ forms t = α·A before its rank-2 step),
+          // so that entries near the under- or overflow limits never meet in a product
+          const cplx cq = cmul(rowq[i], ia), cp = cmul(rowp[i], ia);
           for (int j = lane; j < n; j += 32) {
             cplx v;
-            if (j == p) v = cneg(cmul(rqi, ia));
-            else if (j == q) v = cmul(rpi, ia);
-            else v = cadd(Ai[j], cmul(csub(cmul(rqi, rowp[j]), cmul(rpi, rowq[j])), ia));
+            if (j == p) v = cneg(cq);
+            else if (j == q) v = cp;
+            else v = cadd(Ai[j], csub(cmul(cq, rowp[j]), cmul(cp, rowq[j])));
             Ai[j] = v;
           }
         }
@@ -148,44 +152,38 @@ __global__ void __launch_bounds__(kCplxThreads)
   }
 }
 
-struct Buf {
-  void* p = nullptr;
-  ~Buf() {
-    if (p) cudaFree(p);
-  }
-};
-
 }  // namespace
+
+}  // namespace mvmcb
+
+namespace mvmcb {
+
+// Stream-ordered launch on device buffers: x, inv hold `planes` column-major n×n complex
+// planes as (re, im) doubles, pf `planes` complex values, status one int per plane.
+int pfinv_complex_device(const double* x, int n, int planes, double* pf, double* inv, int* status,
+                         cudaStream_t stream) {
+  if (n <= 0 || (n & 1) || planes < 0) return kErrArgument;
+  if (planes == 0) return kOk;
+  const size_t smem = 2 * sizeof(cplx) * n + sizeof(int) * n;
+  if (smem > static_cast<size_t>(current_device_attr(cudaDevAttrMaxSharedMemoryPerBlockOptin))) return kErrArgument;
+  if (smem > 48 * 1024)
+    MVMCB_CUDA(cudaFuncSetAttribute(k_pfinv_complex, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+  const int sms = current_device_attr(cudaDevAttrMultiProcessorCount);
+  const int grid = std::max(1, std::min(planes, 8 * sms));
+  k_pfinv_complex<<<grid, kCplxThreads, smem, stream>>>(reinterpret_cast<const cplx*>(x), n, planes,
+                                                        reinterpret_cast<cplx*>(inv), reinterpret_cast<cplx*>(pf),
+                                                        status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
 
 }  // namespace mvmcb
 
 using namespace mvmcb;
 
-extern "C" int mvmc_b200_pfinv_batch_complex(const double* x, int n, int planes, double* pf, double* inv,
-                                             int* status) {
-  if (n <= 0 || (n & 1) || planes < 0) return kErrArgument;
-  if (planes == 0) return kOk;
-  if (!x || !pf || !inv || !status) return kErrArgument;
-  const size_t elems = static_cast<size_t>(n) * n * planes;
-  Buf dx, dinv, dpf, dst;
-  MVMCB_CUDA(cudaMalloc(&dx.p, elems * sizeof(cplx)));
-  MVMCB_CUDA(cudaMalloc(&dinv.p, elems * sizeof(cplx)));
-  MVMCB_CUDA(cudaMalloc(&dpf.p, planes * sizeof(cplx)));
-  MVMCB_CUDA(cudaMalloc(&dst.p, planes * sizeof(int)));
-  MVMCB_CUDA(cudaMemcpy(dx.p, x, elems * sizeof(cplx), cudaMemcpyHostToDevice));
-  const size_t smem = 2 * sizeof(cplx) * n + sizeof(int) * n;
-  if (smem > 48 * 1024) MVMCB_CUDA(cudaFuncSetAttribute(k_pfinv_complex, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                        static_cast<int>(smem)));
-  int dev = 0, sms = 0;
-  MVMCB_CUDA(cudaGetDevice(&dev));
-  MVMCB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int grid = std::max(1, std::min(planes, 8 * sms));
-  k_pfinv_complex<<<grid, kCplxThreads, smem>>>(static_cast<const cplx*>(dx.p), n, planes,
-                                                static_cast<cplx*>(dinv.p), static_cast<cplx*>(dpf.p),
-                                                static_cast<int*>(dst.p));
-  MVMCB_CUDA(cudaGetLastError());
-  MVMCB_CUDA(cudaMemcpy(inv, dinv.p, elems * sizeof(cplx), cudaMemcpyDeviceToHost));
-  MVMCB_CUDA(cudaMemcpy(pf, dpf.p, planes * sizeof(cplx), cudaMemcpyDeviceToHost));
-  MVMCB_CUDA(cudaMemcpy(status, dst.p, planes * sizeof(int), cudaMemcpyDeviceToHost));
-  return kOk;
+extern "C" int mvmc_b200_pfinv_batch_complex_device(const double* x, int n, int planes, double* pf, double* inv,
+                                                    int* status, void* stream) {
+  if (planes > 0 && (!x || !pf || !inv || !status)) return kErrArgument;
+  return pfinv_complex_device(x, n, planes, pf, inv, status, static_cast<cudaStream_t>(stream));
 }

@@ -380,18 +380,11 @@ int launch_local_product(const double* oa, long long ns, int na, const double* v
   return kOk;
 }
 
-// One block per SM (co-resident for the cooperative launch).
+// One block per SM of the current device (co-resident for the cooperative launch).
 int cg_grid_blocks(long long ns, int na) {
   (void)ns;
   (void)na;
-  static int sms = -1;
-  if (sms < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    sms = std::max(1, sms);
-  }
-  return sms;
+  return std::max(1, current_device_attr(cudaDevAttrMultiProcessorCount));
 }
 
 int cg_grid_blocks_kind(long long ns, int na, int kind) {

@@ -22,4 +22,5 @@ extern "C" void mvmc_b200_default_options(mvmc_b200_options* opt) {
   opt->device = 0;
   opt->sr_precision = 0;
   opt->refresh_guard = 0.0;
+  opt->c_order = 0;
 }

@@ -27,7 +27,7 @@ EXPORTS = [
     "mvmc_b200_stage_state", "mvmc_b200_gram", "mvmc_b200_cholesky_solve",
     "mvmc_b200_measure_sums", "mvmc_b200_sr_gather", "mvmc_b200_sr_local_product", "mvmc_b200_sr_apply",
     "mvmc_b200_sr_config", "mvmc_b200_physcal_create", "mvmc_b200_green_dims", "mvmc_b200_measure_green",
-    "mvmc_b200_run_physcal", "mvmc_b200_pfinv_batch_complex",
+    "mvmc_b200_run_physcal", "mvmc_b200_pfinv_batch_complex", "mvmc_b200_pfinv_batch_complex_device",
 ]
 
 
@@ -35,7 +35,7 @@ class Options(ctypes.Structure):
     _fields_ = [("walkers", ctypes.c_int), ("precision", ctypes.c_int),
                 ("refresh_sweeps", ctypes.c_int), ("saved_per_walker", ctypes.c_int),
                 ("seed", ctypes.c_longlong), ("device", ctypes.c_int), ("sr_precision", ctypes.c_int),
-                ("refresh_guard", ctypes.c_double)]
+                ("refresh_guard", ctypes.c_double), ("c_order", ctypes.c_int)]
 
 
 def lib():

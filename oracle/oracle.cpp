@@ -746,6 +746,51 @@ void init_walker(const Ctx& c, Walker& w) {
 }
 
 // ===================================================================================
+// exp of the local energy's projection ratios. The reference calls the platform libm
+// (mvmc-expert-parsers/src/utils/c_math.rs): std::exp here. For the bitwise C-order parity
+// gate with the device, oracle_set_fixed_exp(1) switches to fixed_exp: Cody–Waite reduction
+// x = k·ln2 + r (fdlibm's ln2 split, k·ln2_hi exact), the Taylor polynomial of degree 13 in
+// Horner form, 2^k in two exact power-of-two steps; every step one IEEE double operation,
+// so that any host computes the same bits (libm exps differ in the last bit on some
+// arguments; glibc's is not correctly rounded on ~0.1 % of them).
+// ===================================================================================
+bool g_fixed_exp = false;
+
+double pow2i(int e) {
+  const uint64_t bits = static_cast<uint64_t>(e + 1023) << 52;
+  double v;
+  std::memcpy(&v, &bits, sizeof(v));
+  return v;
+}
+
+double fixed_exp(double x) {
+  if (x != x) return x;
+  if (x > 709.782712893384) return std::numeric_limits<double>::infinity();
+  if (x < -745.1332191019412) return 0.0;
+  const double kd = std::floor(x * 0x1.71547652b82fep+0 + 0.5);
+  const int k = static_cast<int>(kd);
+  const double r = (x - kd * 0x1.62e42fee00000p-1) - kd * 0x1.a39ef35793c76p-33;
+  double p = 0x1.6124613a86d09p-33;
+  p = p * r + 0x1.1eed8eff8d898p-29;
+  p = p * r + 0x1.ae64567f544e4p-26;
+  p = p * r + 0x1.27e4fb7789f5cp-22;
+  p = p * r + 0x1.71de3a556c734p-19;
+  p = p * r + 0x1.a01a01a01a01ap-16;
+  p = p * r + 0x1.a01a01a01a01ap-13;
+  p = p * r + 0x1.6c16c16c16c17p-10;
+  p = p * r + 0x1.1111111111111p-7;
+  p = p * r + 0x1.5555555555555p-5;
+  p = p * r + 0x1.5555555555555p-3;
+  p = p * r + 0x1.0000000000000p-1;
+  p = p * r + 1.0;
+  p = p * r + 1.0;
+  const int k1 = k / 2, k2 = k - k1;
+  return (p * pow2i(k1)) * pow2i(k2);
+}
+
+double energy_exp(double z) { return g_fixed_exp ? fixed_exp(z) : std::exp(z); }
+
+// ===================================================================================
 // Measurement (run.rs:2937-3614; observables.rs:202-330,483-560,1553-1760,3447-3610;
 // slater_derivative.rs:75-99,196-430,490-550)
 // ===================================================================================
@@ -789,7 +834,7 @@ double local_energy(const Ctx& c, const int64_t* idx, const int64_t* cfg, const 
         if (site != source && site != dest)
           z += (c.jast_pair[dest * ns + site] - c.jast_pair[source * ns + site]) *
                static_cast<double>(charge(site));
-      const double proj_ratio = std::exp(z);
+      const double proj_ratio = energy_exp(z);
       for (int k = 0; k < n; ++k) rsj[k] = (k == msj ? ri : static_cast<int>(idx[k])) + (k >= ne ? ns : 0);
       const int rsa = ri + s2 * ns;
       double new_ip = 0.0;
@@ -1818,6 +1863,10 @@ int oracle_cholesky_solve(double* a, double* b, int n) {
 }
 
 void oracle_set_refresh_guard(double g) { orc::g_guard = g; }
+
+void oracle_set_fixed_exp(int on) { orc::g_fixed_exp = on != 0; }
+
+double oracle_fixed_exp(double x) { return orc::fixed_exp(x); }
 
 void oracle_refresh_counts(long long* sched, long long* guard, int reset) {
   *sched = orc::g_sched_count;

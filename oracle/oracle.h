@@ -108,6 +108,10 @@ double oracle_refresh_drift(int reset);
 // (0 = off, the reference's schedule). Counts: scheduled and guard refreshes since reset.
 void oracle_set_refresh_guard(double g);
 void oracle_refresh_counts(long long* sched, long long* guard, int reset);
+/* 1: the local energy's projection ratios use fixed_exp (a fixed IEEE operation sequence the
+ * device's C-order mode reproduces bit for bit); 0 (default): the platform libm's exp. */
+void oracle_set_fixed_exp(int on);
+double oracle_fixed_exp(double x);
 
 // The direct SR solve (LAPACK dpotrf('U') + dpotrs order): a is n×n row-major symmetric,
 // overwritten by U (a = UᵀU) in its upper triangle; b becomes x. Returns 0, the 1-based

@@ -117,6 +117,25 @@ def step1_operands(namelist, cg=1, store=0, seed=1):
     return dict(energy=e, ho=ho, oo=oo, o=o)
 
 
+class fixed_exp_mode:
+    """Context in which the oracle's local-energy projection ratios use fixed_exp (the exp
+    the device's C-order mode computes) instead of the platform libm's exp."""
+
+    def __enter__(self):
+        lib().oracle_set_fixed_exp(1)
+        return self
+
+    def __exit__(self, *exc):
+        lib().oracle_set_fixed_exp(0)
+        return False
+
+
+def fixed_exp(x):
+    f = lib().oracle_fixed_exp
+    f.restype, f.argtypes = ctypes.c_double, [ctypes.c_double]
+    return f(float(x))
+
+
 def run_opt(namelist, out_dir, walkers=1, nsteps=0, seed=-1, initial_def=""):
     err = err_buf()
     rc = lib().oracle_run_opt(namelist.encode(), initial_def.encode(), out_dir.encode(), walkers,

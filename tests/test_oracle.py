@@ -160,3 +160,25 @@ def test_direct_sr_optimisation_runs_and_updates(tmp_path):
     info = open(tmp_path / "zvo_SRinfo.dat").read().splitlines()
     assert info[0].split()[-1] == "imax"
     assert len(info) == 4 and all(len(r.split()) == 8 for r in info[1:])
+
+
+def test_fixed_exp_is_within_one_ulp_of_libm():
+    """The exp of the C-order parity mode (Cody–Waite reduction, degree-13 Taylor polynomial,
+    exact 2^k scaling) agrees with the platform libm to one ulp over the arguments the
+    projection ratios take and at the range ends."""
+    import math
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([rng.uniform(-40, 40, 20000), rng.uniform(-1, 1, 20000),
+                         [0.0, -0.0, 1e-300, -1e-300, 700.0, -700.0, -744.0, 709.7]])
+    for x in xs:
+        a, b = ol.fixed_exp(x), math.exp(x)
+        assert abs(a - b) <= math.ulp(b), x
+    assert ol.fixed_exp(0.0) == 1.0 and ol.fixed_exp(800.0) == math.inf and ol.fixed_exp(-800.0) == 0.0
+
+
+def test_fixed_exp_oracle_keeps_its_native_c_pins():
+    """With the fixed exp in the local energy the oracle still meets the native C pins:
+    PhysCal energies (1e-12) and step-1 SR operands (abs 1e-14 / rel 1e-13)."""
+    with ol.fixed_exp_mode():
+        test_physcal_energy_matches_native_c_zvo_out()
+        test_step1_sr_operands_match_native_c()

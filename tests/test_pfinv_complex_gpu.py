@@ -106,3 +106,62 @@ def test_singular_complex_plane_reports_its_pivot_row():
     x[0, 0, 1], x[0, 1, 0] = 1 + 1j, -1 - 1j
     pf, inv, st = mvmc().pfinv_batch_complex(colmajor(x), 4, 1)
     assert st[0] == 3 and pf[0] == 0
+
+
+@pytest.mark.parametrize("scale", [1e-160, 1e160])
+def test_tiny_and_huge_planes_factor_like_the_reference(scale):
+    """Pivots are chosen by |Re| + |Im| (zsktf2's IZAMAX 1-norm) and the update coefficients
+    are scaled by 1/a before they meet another entry, so planes whose entries lie below
+    1e-154 or above 1e154 (where |z|² and products of two entries under- or overflow) still
+    factor: the inverse is the unscaled one times 1/scale. For n = 2 the Pfaffian is scale
+    times the unscaled one; for n = 8 it is scale⁴ (1e-640 underflows to 0 with status 0,
+    1e640 overflows: status -1, the reference's non-finite Pfaffian)."""
+    for n in (2, 8):
+        x = skew_complex(np.random.default_rng(11 + n), n, 3)
+        pf0, inv0, st0 = mvmc().pfinv_batch_complex(colmajor(x), n, 3)
+        pf, inv, st = mvmc().pfinv_batch_complex(colmajor(x * scale), n, 3)
+        assert (st0 == 0).all()
+        want = -1 if (n == 8 and scale > 1) else 0
+        assert (st == want).all(), st
+        assert np.allclose(inv * scale, inv0, rtol=1e-12, atol=1e-12 * np.abs(inv0).max())
+        if n == 2:
+            assert np.allclose(pf, pf0 * scale, rtol=1e-14)
+
+
+def test_device_buffer_entry_matches_the_host_entry():
+    """mvmc_b200_pfinv_batch_complex_device on device buffers (torch allocations, the
+    caller's stream) gives the host-buffer entry point's bits."""
+    import ctypes
+    import torch
+    m = mvmc()
+    n, planes = 24, 40
+    x = colmajor(skew_complex(np.random.default_rng(5), n, planes))
+    pf_h, inv_h, st_h = m.pfinv_batch_complex(x, n, planes)
+    dx = torch.from_numpy(x.view(np.float64).copy()).cuda()
+    dinv = torch.empty_like(dx)
+    dpf = torch.zeros(2 * planes, dtype=torch.float64, device="cuda")
+    dst = torch.zeros(planes, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = m.lib().mvmc_b200_pfinv_batch_complex_device(P(dx), n, planes, P(dpf), P(dinv), P(dst),
+                                                      ctypes.c_void_p(stream.cuda_stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(dpf.cpu().numpy().view(np.complex128), pf_h)
+    assert np.array_equal(dinv.cpu().numpy().view(np.complex128), inv_h)
+    assert np.array_equal(dst.cpu().numpy(), st_h)
+
+
+def test_batch_spanning_several_pipeline_chunks():
+    """480 planes of n = 96 (71 MB, three ~32 MB chunks on the two-stream pipe): every
+    inverse residual at rounding level and Pf² = det on every plane."""
+    n, planes = 96, 480
+    x = skew_complex(np.random.default_rng(17), n, planes)
+    pf, inv, st = mvmc().pfinv_batch_complex(colmajor(x), n, planes)
+    assert (st == 0).all()
+    xi = np.transpose(inv.reshape(planes, n, n), (0, 2, 1))
+    resid = np.abs(xi @ x - np.eye(n)).max(axis=(1, 2))
+    assert resid.max() <= 1e-11 * n
+    sign, logdet = np.linalg.slogdet(x)
+    lpf2 = 2 * np.log(pf)
+    assert np.allclose(np.exp(lpf2 - logdet), sign, rtol=1e-10 * n)

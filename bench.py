@@ -330,6 +330,158 @@ def accuracy_check(args, W, namelist, initial_def, local):
             "refresh_drift_max": drift["drift_max"], "refresh_drift_mean": drift["drift_mean"]}
 
 
+def l2_copy_gbs():
+    """Copy bandwidth of a working set that stays in L2 (2 × 24 MB, read + write bytes, best
+    of 20 after warm-up, CUDA events): the ceiling for a kernel whose planes are L2-resident."""
+    import torch
+    n = 24 * (1 << 20) // 4
+    a = torch.randn(n, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(5):
+        b.copy_(a)
+    best = 1e30
+    for _ in range(20):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 10)
+    return 2 * 4 * n / (best / 1e3) / 1e9
+
+
+def sr16_record(args, local, timed=3):
+    """The 2D 16×16 SR workload (t' = -0.2, U = 6, 112 + 112 electrons, n = 224, 4×4-sublattice
+    f: 4226 parameters, 8192 walkers, SR-CG): SR-step time split into sampling, measurement
+    and SR-CG for the plain FP64 path and the mixed path (FP32 inverse updates with FP64
+    refresh, BF16 centred column-scaled SR operator), and the mixed path's errors on the first
+    step from the same seeds and parameters: energy per site, variance, <O_k> and the SR
+    parameter update; the update error of the BF16 operator alone on the FP64 path's samples."""
+    import torch
+    import lattice
+    import mvmc_b200 as mb
+    cfg = dict(lattice.CONFIGS["square16_sr"])
+    tmp = tempfile.mkdtemp(prefix="mvmc_sr16_")
+    nl, init, dims = lattice.write_inputs(os.path.join(tmp, "in"), **cfg)
+    W = WALKERS["square16_sr"]
+
+    def run(precision, sr_precision, steps):
+        eng = mb.Engine(nl, init, walkers=W, precision=precision, seed=12345,
+                        refresh_sweeps=args.refresh if precision == 32 else 0,
+                        refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision)
+        stream = torch.cuda.ExternalStream(eng.stream())
+        p0 = eng.parameters()
+        eng.sample()
+        e, ho, oo = eng.measure()
+        idx = eng.samples()["ele_idx"].reshape(W, -1)
+        eng.sr_cg()
+        first = {"e": e, "oo": oo, "dp": eng.parameters() - p0, "idx": idx}
+        if steps == 0:
+            eng.close()
+            return first, None
+        split = []
+        for k in range(1 + steps):  # one untimed warm step, then the timed ones
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(stream)
+            eng.sample()
+            ev[1].record(stream)
+            eng.measure()
+            ev[2].record(stream)
+            eng.sr_cg()
+            ev[3].record(stream)
+            torch.cuda.synchronize()
+            if k:
+                split.append([ev[i].elapsed_time(ev[i + 1]) for i in range(3)])
+        eng.close()
+        s = np.mean(np.array(split), axis=0)
+        return first, {"sample_ms": float(s[0]), "measure_ms": float(s[1]), "sr_cg_ms": float(s[2]),
+                       "sr_step_ms": float(s.sum())}
+
+    a_first, a_t = run(64, 64, timed)
+    c_first, c_t = run(32, 16, timed)
+    b_first, _ = run(64, 16, 0)
+    ns = dims["nsite"]
+    size = 1 + dims["npara"]
+    var = lambda f: float(f["e"][2] - f["e"][1] ** 2)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    return {
+        "workload": "square16_sr", "walkers": W, "n": dims["n"], "npara": dims["npara"],
+        "sweeps_per_walker_step": (cfg["samples"] + 1) * cfg["interval"],
+        "fp64": a_t, "mixed": c_t,
+        "mixed_over_fp64": {"sr_step": a_t["sr_step_ms"] / c_t["sr_step_ms"],
+                            "sweeps": a_t["sample_ms"] / c_t["sample_ms"],
+                            "measure": a_t["measure_ms"] / c_t["measure_ms"],
+                            "sr_cg": a_t["sr_cg_ms"] / c_t["sr_cg_ms"]},
+        "mixed_precision": {"sampler": "f32 updates + f64 refresh", "refresh_sweeps": args.refresh,
+                            "refresh_guard": args.guard, "sr_operator": "bf16 centred, column-scaled"},
+        "accuracy_first_step": {
+            "identical_chains": float(np.mean(np.all(a_first["idx"] == c_first["idx"], axis=1))),
+            "dE_per_site": float(abs(c_first["e"][1] - a_first["e"][1]) / ns),
+            "variance_fp64": var(a_first), "dvariance": abs(var(c_first) - var(a_first)),
+            "max_dO_mean": float(np.max(np.abs(c_first["oo"][:size] - a_first["oo"][:size]))),
+            "update_rel_err_mixed": rel(c_first["dp"], a_first["dp"]),
+            "update_rel_err_bf16_operator_only": rel(b_first["dp"], a_first["dp"])},
+    }
+
+
+def pfinv_records(local, steps=10, warmup=3):
+    """Batched Pfaffian + inverse on device buffers: B = 8192 planes of n = 64 and the
+    five-size mix {32, 48, 64, 96, 128} (8190 planes), FP64 and FP32 sweeps: planes/s and
+    the fraction of the measured cuBLAS FP64 GEMM rate (2n³ flops per plane)."""
+    import ctypes
+    import torch
+    import mvmc_b200 as mb
+    L = mb.lib()
+    peak = fp64_gemm_peak()
+    out = {"fp64_gemm_tflops": peak}
+    for name in ("pfinv64", "pfinv_mix"):
+        sizes = PFINV[name]
+        rng = np.random.default_rng(2024)
+        uniq = sorted(set(sizes))
+        by_n = {n: skew_planes(rng, n, sizes.count(n)) for n in uniq}
+        cur = {n: 0 for n in uniq}
+        chunks = []
+        for n in sizes:
+            chunks.append(by_n[n][cur[n]].ravel())
+            cur[n] += 1
+        x = torch.from_numpy(np.concatenate(chunks)).cuda()
+        inv = torch.empty_like(x)
+        B = len(sizes)
+        pf = torch.zeros(B, dtype=torch.float64, device="cuda")
+        st = torch.zeros(B, dtype=torch.int32, device="cuda")
+        szs = np.asarray(sizes, dtype=np.int32)
+        sz = torch.from_numpy(szs).cuda()
+        off = torch.from_numpy(np.concatenate([[0], np.cumsum(szs.astype(np.int64) ** 2)[:-1]])).cuda()
+        uniform = len(uniq) == 1
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        stream = torch.cuda.current_stream()
+        rec = {"planes": B, "sizes": uniq}
+        for prec in (64, 32):
+            def launch():
+                rc = L.mvmc_b200_pfinv_batch_device(P(x), None if uniform else P(sz), None if uniform else P(off),
+                                                    uniq[0] if uniform else 0, B, max(uniq), P(pf), P(inv), P(st),
+                                                    prec, ctypes.c_void_p(stream.cuda_stream))
+                if rc < 0:
+                    raise RuntimeError(L.mvmc_b200_last_error().decode())
+            for _ in range(warmup):
+                launch()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                launch()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            flops = float(sum(2 * n ** 3 for n in sizes))
+            rec[f"fp{prec}"] = {"planes_per_s": B / (ms / 1e3), "ms": ms, "tflops": flops / (ms / 1e3) / 1e12,
+                                "frac_of_fp64_gemm": flops / (ms / 1e3) / 1e12 / peak,
+                                "singular": int((st != 0).sum())}
+        out[name] = rec
+        del x, inv
+    return out
+
+
 def engine_bench(args, ws, rank, local):
     import torch
     dist = None
@@ -405,6 +557,8 @@ def engine_bench(args, ws, rank, local):
                 "h2d_bytes_per_step": main_rec["h2d"] // args.steps,
                 "d2h_bytes_per_step": main_rec["d2h"] // args.steps},
         "gpu_launches": 8 * args.steps,
+        "headline": ("plain FP64 path" if args.precision == 64 else "mixed path") +
+                    "; the other path is timed beside it with its measured error against FP64",
         "residency": os.environ.get("MVMC_B200_RESIDENCY", "auto"),
         "clocks": summarize_clocks(clocks_path, local),
     }
@@ -424,6 +578,15 @@ def engine_bench(args, ws, rank, local):
             out["accuracy"]["dE_per_site"] = acc["dE"] / ns
     if os.environ.get("MVMC_B200_TIMERS") == "1":
         out["timers"] = "phase cycles: run the engine directly for mvmc_b200_sampler_timers"
+    if not args.no_extra and args.config == "square8" and ws == 1:
+        # the sampler's planes are served from L2: its effective bandwidth against a measured
+        # L2-resident copy as well as against HBM
+        l2 = l2_copy_gbs()
+        out["roofline"]["l2_peak"] = l2
+        out["roofline"]["l2_frac"] = achieved / l2
+        out["roofline"]["l2_peak_kind"] = "measured: torch copy of a 2 x 24 MB working set in this run"
+        out["square16_sr"] = sr16_record(args, local)
+        out["pfinv"] = pfinv_records(local)
     print(json.dumps(out), flush=True)
     if ws > 1:
         dist.destroy_process_group()
@@ -748,6 +911,8 @@ def main():
     ap.add_argument("--sr-precision", type=int, default=0, choices=(0, 64, 32, 16),
                     help="SR operator storage of the timed engine (0: FP64)")
     ap.add_argument("--direct", action="store_true", help="direct SR (NSRCG 0): Gram + Cholesky instead of SR-CG")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="square8: skip the 16x16 SR-step record, the Pfaffian records and the L2 ceiling")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     ws, rank, local = dist_env()

@@ -4,8 +4,10 @@
 // and HostEngine::run_block (sampling/engine.rs:188-476) of AtelierArith/mvmc-rs for the
 // real sz-conserved path, with C's exact draw contract:
 //   get_update_type (candidate.rs:320), make_candidate_hopping / _exchange
-//   (candidate.rs:137,230), update_ele_config / update_proj_cnt / log_proj_ratio
-//   (projection.rs:278,403,418,441), metropolis_decision (metropolis.rs:42-83), the
+//   (candidate.rs:137,230), update_ele_config (projection.rs:418,441), log_proj_ratio
+//   (projection.rs:403; for a hop in the direct-table form of the local energy's
+//   projection ratio, exactly 0 for an exchange, with the counters rebuilt from the
+//   configuration where a sample is saved), metropolis_decision (metropolis.rs:42-83), the
 //   Pfaffian ratios and rank-2 / rank-4 updates (updates.rs:73,395,588,779,1154,1429),
 //   and the refresh when the accept window exceeds Nsite (engine.rs:454-474).
 // Thread 0 runs the serial Markov-chain logic from the walker's SFMT state in shared
@@ -27,7 +29,7 @@ namespace mvmcb {
 
 
 struct SampLayout {
-  size_t sf, ctl, dctl, idx, cfg, num, cnt, cntn, cntm, pf, pfn, proj, qpw, jidx, vec, gj, ws, planes, total;
+  size_t sf, ctl, dctl, idx, cfg, num, cnt, pf, pfn, proj, qpw, jidx, vec, gj, ws, planes, total;
 };
 
 // The Jastrow index table is staged in shared memory for lattices up to this many sites.
@@ -46,8 +48,6 @@ __host__ __device__ inline SampLayout samp_layout(const DevModel& m, bool smem_p
   L.cfg = o; o = align16(o + sizeof(int) * m.ns2);
   L.num = o; o = align16(o + sizeof(int) * m.ns2);
   L.cnt = o; o = align16(o + sizeof(int) * (m.nproj + 1));
-  L.cntn = o; o = align16(o + sizeof(int) * (m.nproj + 1));
-  L.cntm = o; o = align16(o + sizeof(int) * (m.nproj + 1));
   L.pf = o; o = align16(o + sizeof(double) * m.nqp);
   L.pfn = o; o = align16(o + sizeof(double) * m.nqp);
   L.proj = o; o = align16(o + sizeof(double) * (m.nproj + 1));
@@ -74,21 +74,12 @@ enum Ctl {
 };
 enum DCtl { dLogIp = 0, dLogIpNew = 1, dDproj = 2 };
 
-// Δ ln P = Σ_k α_k (c'_k − c_k) by one warp (log_proj_ratio, projection.rs:403).
-__device__ __forceinline__ double log_proj_ratio_warp(int nproj, const double* proj, const int* cnew,
-                                                      const int* cold) {
-  const int lane = threadIdx.x & 31;
-  double z = 0.0;
-  for (int k = lane; k < nproj; k += 32) z += proj[k] * static_cast<double>(cnew[k] - cold[k]);
-  return warp_sum(z);
-}
-
 template <typename T>
 struct WalkerSmem {
   uint32_t* sf;
   int* ctl;
   double* dctl;
-  int *idx, *cfg, *num, *cnt, *cntn, *cntm;
+  int *idx, *cfg, *num, *cnt;
   double *pf, *pfn, *proj, *qpw;
   const int* jidx; // Jastrow index table (shared memory when small, else global)
   T* vec;          // [nqp][4][n]
@@ -134,37 +125,61 @@ __device__ void make_proj_cnt_serial(const DevModel& m, const int* num, int* cnt
     }
 }
 
-// update_proj_cnt by one warp; `num` accessor gives the occupation after the move.
-template <typename NumFn>
-__device__ void update_proj_cnt_warp(const DevModel& m, const int* jtab, int ri, int rj, int* cnew,
-                                     const int* cold, NumFn num) {
-  const int lane = threadIdx.x & 31;
-  for (int k = lane; k < m.nproj; k += 32) cnew[k] = cold[k];
-  __syncwarp();
-  if (ri == rj) return;
-  const int ns = m.ns;
-  if (lane == 0 && m.n_gutz > 0) {
-    const int gi = m.gutz_idx[ri], gj = m.gutz_idx[rj];
-    if (gi >= 0 && gi < m.nproj) atomicAdd(cnew + gi, -(num(ri) + num(ri + ns)));
-    if (gj >= 0 && gj < m.nproj) atomicAdd(cnew + gj, num(rj) * num(rj + ns));
-  }
+// Δ ln P of a hop from `source` to `dest` by one warp, `num` holding the configuration
+// after the move: the direct-table form of Σ_k α_k (c'_k − c_k) (gutz_site[r] = α of r's
+// Gutzwiller class, jast_pair[a·ns + b] = α of the Jastrow class of (a, b); the form of the
+// local energy's projection ratio, observables.rs:1553-1640):
+//   − g(source)·n(source) + g(dest)·n↑n↓(dest) + v(source, dest)·(x'_source − x'_dest + 1)
+//   + Σ_{k ≠ source, dest} (v(dest, k) − v(source, k))·x_k,   x = n↑ + n↓ − 1.
+// Mathematically the counters' sum; the projection counters themselves are not needed
+// while the walker moves and are rebuilt from the configuration where a sample is saved.
+__device__ __forceinline__ double log_proj_ratio_hop_warp(const DevModel& m, const int* num, int source, int dest) {
+  const int lane = threadIdx.x & 31, ns = m.ns;
+  double z = 0.0;
   if (m.n_jast > 0) {
-    const int off = m.n_gutz;
-    auto jidx = [&](int a, int b) { return jtab[min(a, b) * ns + max(a, b)]; };
-    if (lane == 0) {
-      const int ij = jidx(ri, rj);
-      if (ij >= 0) atomicAdd(cnew + off + ij, (num(ri) + num(ri + ns)) - (num(rj) + num(rj + ns)) + 1);
+    const double* vd = m.jast_pair + static_cast<size_t>(dest) * ns;
+    const double* vs = m.jast_pair + static_cast<size_t>(source) * ns;
+    for (int k = lane; k < ns; k += 32) {
+      if (k == source || k == dest) continue;
+      const int x = num[k] + num[k + ns] - 1;
+      if (x != 0) z += (__ldg(vd + k) - __ldg(vs + k)) * static_cast<double>(x);
     }
-    for (int rk = lane; rk < ns; rk += 32) {
-      if (rk == ri || rk == rj) continue;
-      const int xk = num(rk) + num(rk + ns) - 1;
-      if (xk == 0) continue;
-      const int ik = jidx(ri, rk), jk = jidx(rj, rk);
-      if (ik >= 0) atomicAdd(cnew + off + ik, -xk);
-      if (jk >= 0) atomicAdd(cnew + off + jk, xk);
-    }
+    z = warp_sum(z);
   }
-  __syncwarp();
+  if (lane == 0) {
+    const int xs = num[source] + num[source + ns] - 1, xd = num[dest] + num[dest + ns] - 1;
+    z -= __ldg(m.gutz_site + source) * static_cast<double>(num[source] + num[source + ns]);
+    z += __ldg(m.gutz_site + dest) * static_cast<double>(num[dest] * num[dest + ns]);
+    z += __ldg(m.jast_pair + static_cast<size_t>(source) * ns + dest) * static_cast<double>(xs - xd + 1);
+  }
+  return z;
+}
+
+// Projection counters from the configuration by the whole CTA (make_proj_cnt,
+// projection.rs:179): integer sums, so the order of the atomics does not matter.
+__device__ void make_proj_cnt_cta(const DevModel& m, const int* jtab, const int* num, int* cnt) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  const int ns = m.ns;
+  for (int k = tid; k < m.nproj; k += nt) cnt[k] = 0;
+  __syncthreads();
+  if (m.n_gutz > 0)
+    for (int r = tid; r < ns; r += nt) {
+      const int g = m.gutz_idx[r];
+      const int v = num[r] * num[r + ns];
+      if (v && g >= 0 && g < m.nproj) atomicAdd(cnt + g, v);
+    }
+  if (m.n_jast > 0)
+    for (int ri = warp; ri < ns; ri += nwarp) {
+      const int xi = num[ri] + num[ri + ns] - 1;
+      if (xi == 0) continue;
+      for (int rj = ri + 1 + lane; rj < ns; rj += 32) {
+        const int j = jtab[ri * ns + rj];
+        if (j < 0) continue;
+        const int xj = num[rj] + num[rj + ns] - 1;
+        if (xj != 0 && m.n_gutz + j < m.nproj) atomicAdd(cnt + m.n_gutz + j, xi * xj);
+      }
+    }
+  __syncthreads();
 }
 
 // ---- CalculateMAll on every plane (CTA-wide); returns 0 ok, else the first failure -------
@@ -226,7 +241,10 @@ template <typename T>
 __device__ void ratio_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa) {
   const int n = m.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int rsa = rs_of(m, s.idx, msa);
-  for (int q = warp; q < m.nqp; q += nwarp) {
+  // warps 1.. take the planes (warp 0 updates the projection counters meanwhile)
+  const int pw = nwarp > 1 ? nwarp - 1 : 1, wi = nwarp > 1 ? warp - 1 : warp;
+  if (wi < 0) return;
+  for (int q = wi; q < m.nqp; q += pw) {
     const T* row = s.planes + (static_cast<size_t>(q) * n + msa) * n;
     T r = T(0);
     for (int j = lane; j < n; j += 32) r += row[j] * slater_at<T>(m, q, rsa, rs_of(m, s.idx, j));
@@ -282,19 +300,24 @@ __device__ __forceinline__ void col_dot_pair(const T* __restrict__ P0, const T* 
 }
 
 // Column range [i0, i1) of col_dot.
+// Eight independent accumulators: eight row loads in flight per thread (planes in L2 are
+// latency bound at four).
 template <typename T>
 __device__ __forceinline__ T col_dot_range(const T* __restrict__ P, const T* __restrict__ v, int n, int i0,
                                            int i1) {
-  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+  T a[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) a[u] = T(0);
   int i = i0;
-  for (; i + 4 <= i1; i += 4) {
-    a0 += P[(i + 0) * n] * v[i + 0];
-    a1 += P[(i + 1) * n] * v[i + 1];
-    a2 += P[(i + 2) * n] * v[i + 2];
-    a3 += P[(i + 3) * n] * v[i + 3];
+  for (; i + 8 <= i1; i += 8) {
+    T x[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) x[u] = P[(i + u) * n];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] += x[u] * v[i + u];
   }
-  for (; i < i1; ++i) a0 += P[i * n] * v[i];
-  return (a0 + a1) + (a2 + a3);
+  for (; i < i1; ++i) a[0] += P[i * n] * v[i];
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
 }
 
 // out[q][j] = −Σ_i P_q[i][j]·vec[q][in][i] → vec[q][out] for every (plane, column), two
@@ -405,8 +428,9 @@ __device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int ms
     }
     T* P = s.planes + static_cast<size_t>(q) * n * n;
     // rows per batch (their loads are issued before any store), fewer for wide rows so
-    // that several walkers fit an SM's register file
-    constexpr int RB = JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1);
+    // that several walkers fit an SM's register file; two for the widest rows, whose
+    // planes live in L2 where one batch of seven loads leaves the SM latency bound
+    constexpr int RB = JPL <= 2 ? 4 : 2;
     for (int i0 = warp; i0 < n; i0 += nwarp * RB) {
       T x[RB][JPL];
 #pragma unroll
@@ -682,8 +706,6 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
   s.cfg = reinterpret_cast<int*>(smem + L.cfg);
   s.num = reinterpret_cast<int*>(smem + L.num);
   s.cnt = reinterpret_cast<int*>(smem + L.cnt);
-  s.cntn = reinterpret_cast<int*>(smem + L.cntn);
-  s.cntm = reinterpret_cast<int*>(smem + L.cntm);
   s.pf = reinterpret_cast<double*>(smem + L.pf);
   s.pfn = reinterpret_cast<double*>(smem + L.pfn);
   s.proj = reinterpret_cast<double*>(smem + L.proj);
@@ -721,8 +743,9 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
     s.proj[k] = m.proj[k];
   }
   for (int k = tid; k < m.nqp; k += blockDim.x) s.qpw[k] = m.qpw[k];
-  __shared__ int sf_idx;
-  __shared__ unsigned long long sf_draws;
+  // the generator's cursor and word count live in thread 0's registers (only thread 0 draws)
+  int sf_idx = 0;
+  unsigned long long sf_draws = 0;
   if (tid == 0) {
     sf_idx = w.sfmt_idx[wk];
     sf_draws = w.draws[wk];
@@ -865,25 +888,17 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
       if (cc[cSkip]) continue;
       const int type = cc[cType];
       const int ri = cc[cRi], rj = cc[cRj], sp = cc[cS], msa = cc[cMsa];
-      // --- projection counters (warp 0) and Pfaffian ratios (CTA) ---
+      // --- Δ ln P (warp 0) and Pfaffian ratios (CTA) ---
       if (type == 0) {
         if (tid < 32) {
-          update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntn, s.cnt, [&](int k) { return s.num[k]; });
-          const double z = log_proj_ratio_warp(m.nproj, s.proj, s.cntn, s.cnt);
+          const double z = log_proj_ratio_hop_warp(m, s.num, ri, rj);
           if (tid == 0) s.dctl[dDproj] = z;
         }
         ratio_hop_dev<T>(m, s, msa);
       } else {
-        const int t = cc[cT];
-        if (tid < 32) {
-          // first move uses the occupation before the partner's move
-          const int a = rj + t * ns, b = ri + t * ns;
-          auto num_mid = [&](int k) { return k == a ? 1 : (k == b ? 0 : s.num[k]); };
-          update_proj_cnt_warp(m, s.jidx, ri, rj, s.cntm, s.cnt, num_mid);
-          update_proj_cnt_warp(m, s.jidx, rj, ri, s.cntn, s.cntm, [&](int k) { return s.num[k]; });
-          const double z = log_proj_ratio_warp(m.nproj, s.proj, s.cntn, s.cnt);
-          if (tid == 0) s.dctl[dDproj] = z;
-        }
+        // an exchange keeps every site's charge and double occupancy: every projection
+        // counter is unchanged and Σ_k α_k (c'_k − c_k) is exactly 0
+        if (tid == 0) s.dctl[dDproj] = 0.0;
         ratio_exchange_dev<T, JPL>(m, s, msa, cc[cMsb]);
       }
       __syncthreads();
@@ -900,10 +915,10 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
         const int acc = wgt > u ? 1 : 0;
         int guard = 0;
         if (acc) {
-          for (int k = 0; k < m.nproj; ++k) s.cnt[k] = s.cntn[k];
           s.dctl[dLogIp] = lip_new;
           ++n_acc_win;
-          counter[type == 0 ? 1 : 3]++;
+          if (type == 0) counter[1]++;
+          else counter[3]++;
           if (w.refresh_guard > 0.0) {
             // a plane whose Pfaffian ratio leaves [g, 1/g] passes near a singular matrix:
             // the rank-2 update amplifies the inverse's rounding error by about 1/|ratio|
@@ -960,6 +975,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
       }
     }
     if (out + S >= n_out) {
+      make_proj_cnt_cta(m, s.jidx, s.num, s.cnt);
       const size_t sample = static_cast<size_t>(wk) * S + (out + S - n_out);
       for (int k = tid; k < n; k += blockDim.x) w.s_idx[sample * n + k] = s.idx[k];
       for (int k = tid; k < m.ns2; k += blockDim.x) {
@@ -970,6 +986,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
     }
   }
   __syncthreads();
+  make_proj_cnt_cta(m, s.jidx, s.num, s.cnt);
   // ---- store the walker (the final configuration is the burn-in state of the next step) ----
   for (int k = tid; k < kSfmtN32; k += blockDim.x) w.sfmt[static_cast<size_t>(wk) * kSfmtN32 + k] = s.sf[k];
   for (int k = tid; k < n; k += blockDim.x) w.ele_idx[static_cast<size_t>(wk) * n + k] = s.idx[k];

@@ -394,6 +394,37 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   dm.trans = c->upload(trans);
   dm.trans_sgn = c->upload(trans_sgn);
   dm.spgl = c->upload(spgl);
+  // Slater-derivative site pairs by orbital (deterministic O_k of the packed measurement)
+  {
+    std::vector<std::vector<int>> by_orb(std::max(0, m.n_orb));
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b < ns; ++b) {
+        const int k = m.orb_idx[a * ns + b];
+        if (k < 0 || k >= m.n_orb) continue;
+        by_orb[k].push_back((a << 16) | (b << 1) | (m.orb_sgn[a * ns + b] < 0 ? 1 : 0));
+      }
+    std::vector<int> off(1, 0), ent;
+    for (const auto& v : by_orb) {
+      ent.insert(ent.end(), v.begin(), v.end());
+      off.push_back(static_cast<int>(ent.size()));
+    }
+    std::vector<int> tinv(trans.size(), -1);
+    bool perm = true;
+    for (int mp = 0; mp < dm.nmp && perm; ++mp)
+      for (int r = 0; r < ns; ++r) {
+        const int t = trans[mp * ns + r];
+        if (t < 0 || t >= ns || tinv[mp * ns + t] >= 0) {
+          perm = false;
+          break;
+        }
+        tinv[mp * ns + t] = r;
+      }
+    if (!ent.empty() && perm) {
+      dm.orb_off = c->upload(off);
+      dm.orb_ent = c->upload(ent);
+      dm.trans_inv = c->upload(tinv);
+    }
+  }
   dm.tterm = c->upload(tterm);
   dm.tval = c->upload(tval);
   dm.intra_i = c->upload(intra_i);

@@ -48,6 +48,13 @@ struct DevModel {
   int gdense = 0;
   const int* gterm_of = nullptr;
   const int* gfirst = nullptr;
+  // Slater-derivative site pairs by orbital: the translated site pairs (a', b') with
+  // orb_idx[a'·ns + b'] = k are orb_ent[orb_off[k] .. orb_off[k+1]), packed as
+  // (a' << 16) | (b' << 1) | (orb_sgn < 0); trans_inv[mp·ns + a'] is the site a with
+  // translation mp mapping a to a' (null when a translation is not a permutation).
+  const int* orb_off = nullptr;
+  const int* orb_ent = nullptr;
+  const int* trans_inv = nullptr;
   const int* gone = nullptr;  // [ngone*4]: i, s, j, t of c†_{i s} c_{j t}
   const int* gtwo = nullptr;  // [ngtwo*8]: ri, rj, rk, rl, s, u, ref, gen
   const int* ggen = nullptr;  // [nggen*6]: ri, rj, rk, rl, s, u of the two-hop terms

@@ -17,8 +17,9 @@
 // index-coincidence reductions or the two-hop ratio (green_func2, observables.rs:664-860;
 // two_ratio_real, sampling/updates.rs:1539-1567).
 // The reductions sum per walker in sample order and then across walkers in walker
-// order (the rank-order fold of ThreadReducer, multichain.rs:433), so reruns are
-// bitwise repeatable up to the O_k scatter (shared-memory atomics).
+// order (the rank-order fold of ThreadReducer, multichain.rs:433), and the Slater
+// derivative is gathered per orbital in a fixed order, so reruns are bitwise repeatable
+// (a model whose translations are not permutations falls back to an atomic scatter).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -479,15 +480,45 @@ __global__ void __launch_bounds__(NT, (kSmemPlane || NT > kMeasThreads ? 1 : 2))
       }
       __syncthreads();
       const double cs = pfv * m.spgl[spidx], cc = pfv * m.spgl[m.nleg + spidx], ss = pfv * m.spgl[2 * m.nleg + spidx];
-      for (int k = tid; k < n * n; k += nt) {
-        const int i = k / n, j = k - i * n;
-        const int orb = __ldg(m.orb_idx + tr[i] * ns + tr[j]);
-        if (orb < 0 || orb >= m.norb) continue;
-        const int sign = sg[i] * sg[j] * __ldg(m.orb_sgn + tr[i] * ns + tr[j]);
-        const double first = i < ne ? cs : ss, second = i < ne ? cc : cs;
-        const double v = A[k];
-        const double value = j < ne ? v * first : -v * second;
-        atomicAdd(oacc + orb, wq * (value * static_cast<double>(sign)));
+      if (m.orb_off && m.trans_inv) {
+        // by orbital: thread k adds the electron pairs on orbital k's translated site pairs in
+        // a fixed order, so the O row is bitwise repeatable (no atomics)
+        const int* tinv = m.trans_inv + mpidx * ns;
+        const int* tsgn = m.trans_sgn + mpidx * ns;
+        const double fac[4] = {cs, -cc, ss, -cs};  // (up, up), (up, dn), (dn, up), (dn, dn)
+        for (int k = tid; k < m.norb; k += nt) {
+          double acc = 0.0;
+          const int e1 = __ldg(m.orb_off + k + 1);
+          for (int e = __ldg(m.orb_off + k); e < e1; ++e) {
+            const int ent = __ldg(m.orb_ent + e);
+            const int a = __ldg(tinv + (ent >> 16)), b = __ldg(tinv + ((ent >> 1) & 0x7fff));
+            const int sgn = (ent & 1 ? -1 : 1) * __ldg(tsgn + a) * __ldg(tsgn + b);
+#pragma unroll
+            for (int sa = 0; sa < 2; ++sa) {
+              const int ei = cfg[a + sa * ns];
+              if (ei < 0) continue;
+#pragma unroll
+              for (int sb = 0; sb < 2; ++sb) {
+                const int ej = cfg[b + sb * ns];
+                if (ej < 0) continue;
+                acc += (fac[2 * sa + sb] * A[static_cast<size_t>(ei + sa * ne) * n + ej + sb * ne]) *
+                       static_cast<double>(sgn);
+              }
+            }
+          }
+          oacc[k] += wq * acc;
+        }
+      } else {
+        for (int k = tid; k < n * n; k += nt) {
+          const int i = k / n, j = k - i * n;
+          const int orb = __ldg(m.orb_idx + tr[i] * ns + tr[j]);
+          if (orb < 0 || orb >= m.norb) continue;
+          const int sign = sg[i] * sg[j] * __ldg(m.orb_sgn + tr[i] * ns + tr[j]);
+          const double first = i < ne ? cs : ss, second = i < ne ? cc : cs;
+          const double v = A[k];
+          const double value = j < ne ? v * first : -v * second;
+          atomicAdd(oacc + orb, wq * (value * static_cast<double>(sign)));
+        }
       }
       __syncthreads();
     }
@@ -568,6 +599,268 @@ __global__ void __launch_bounds__(NT, (kSmemPlane || NT > kMeasThreads ? 1 : 2))
     }
     __syncthreads();
   }
+}
+
+// ---- planes whose strict upper triangle fits shared memory -----------------------------
+// For n where the full FP64 plane does not fit one SM (2D 16×16, n = 224: 401 KB) the
+// sample's plane is swept as a packed upper triangle in shared memory (gj_pfinv_packed,
+// 195 KB at n = 224), one 512-thread CTA per SM striding over the samples; nothing of the
+// sweep touches L2. The transfer terms' per-term sums sit in the block's L2 workspace. The
+// Slater derivative is gathered per orbital: thread k walks orbital k's translated site
+// pairs in a fixed order and adds the electron pairs on them, so O rows are bitwise
+// repeatable (no atomics).
+struct PackedLayout {
+  size_t idx, cfg, num, cnt, tr, tsg, pf, cj, rs, rowp, rowq, plane, total;
+};
+
+__host__ __device__ inline PackedLayout packed_layout(const DevModel& m) {
+  PackedLayout L;
+  size_t o = 0;
+  L.idx = o; o = a16(o + sizeof(int) * m.n);
+  L.cfg = o; o = a16(o + sizeof(int) * m.ns2);
+  L.num = o; o = a16(o + sizeof(int) * m.ns2);
+  L.cnt = o; o = a16(o + sizeof(int) * (m.nproj + 1));
+  L.tr = o; o = a16(o + sizeof(int) * m.ns);
+  L.tsg = o; o = a16(o + sizeof(int) * m.ns);
+  L.pf = o; o = a16(o + sizeof(double) * (m.nqp + 2));
+  L.cj = o; o = a16(o + sizeof(double) * m.ns);
+  L.rs = o; o = a16(o + sizeof(int) * m.n);
+  L.rowp = o; o = a16(o + 2 * sizeof(double) * m.n);
+  L.rowq = o; o = a16(o + sizeof(double) * m.n);
+  L.plane = o; o = a16(o + sizeof(double) * static_cast<size_t>(m.n) * (m.n - 1) / 2);
+  L.total = o;
+  return L;
+}
+
+constexpr int kPackedThreads = 512;
+
+template <int JPL>
+__global__ void __launch_bounds__(kPackedThreads, 1)
+    k_measure_packed(DevModel m, const int* __restrict__ s_idx, const int* __restrict__ s_cfg,
+                     const int* __restrict__ s_num, const int* __restrict__ s_cnt, int nsamples,
+                     double* __restrict__ gws, size_t gws_stride, double* __restrict__ ostore,
+                     double* __restrict__ eloc, double* __restrict__ lpsi, int* __restrict__ valid, unsigned* status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const PackedLayout L = packed_layout(m);
+  int* idx = reinterpret_cast<int*>(smem + L.idx);
+  int* cfg = reinterpret_cast<int*>(smem + L.cfg);
+  int* num = reinterpret_cast<int*>(smem + L.num);
+  int* cnt = reinterpret_cast<int*>(smem + L.cnt);
+  int* tinv = reinterpret_cast<int*>(smem + L.tr);
+  int* tsg = reinterpret_cast<int*>(smem + L.tsg);
+  double* pf = reinterpret_cast<double*>(smem + L.pf);
+  double* cj = reinterpret_cast<double*>(smem + L.cj);
+  int* rs = reinterpret_cast<int*>(smem + L.rs);
+  double* rowp = reinterpret_cast<double*>(smem + L.rowp);
+  double* rowq = reinterpret_cast<double*>(smem + L.rowq);
+  double* P = reinterpret_cast<double*>(smem + L.plane);
+  const int n = m.n, ns = m.ns, ne = m.ne, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  double* tacc = gws + static_cast<size_t>(blockIdx.x) * gws_stride;  // [nterm] plane sums
+  double* g1 = tacc + m.nterm;                                          // [nterm] term values
+  __shared__ int s_bad;
+  for (int i = tid; i < n; i += nt) rs[i] = i * n - i * (i + 1) / 2 - i - 1;
+
+  for (int sample = blockIdx.x; sample < nsamples; sample += gridDim.x) {
+    for (int k = tid; k < n; k += nt) idx[k] = s_idx[static_cast<size_t>(sample) * n + k];
+    for (int k = tid; k < m.ns2; k += nt) {
+      cfg[k] = s_cfg[static_cast<size_t>(sample) * m.ns2 + k];
+      num[k] = s_num[static_cast<size_t>(sample) * m.ns2 + k];
+    }
+    for (int k = tid; k < m.nproj; k += nt) cnt[k] = s_cnt[static_cast<size_t>(sample) * m.nproj + k];
+    for (int k = tid; k < m.nterm; k += nt) tacc[k] = 0.0;
+    double* orow = ostore + static_cast<size_t>(sample) * m.sr_size;
+    for (int k = tid; k < m.norb; k += nt) orow[1 + m.nproj + k] = 0.0;
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    for (int r = tid; r < ns; r += nt) {  // cj[r] = Σ_site J[r][site]·(n_site − 1)
+      double acc = 0.0;
+      for (int site = 0; site < ns; ++site)
+        acc += __ldg(m.jast_pair + r * ns + site) * static_cast<double>(num[site] + num[site + ns] - 1);
+      cj[r] = acc;
+    }
+    if (tid == 0) {
+      bool all_zero = true, all_neg = true;
+      for (int k = 0; k < n; ++k) {
+        all_zero = all_zero && idx[k] == 0;
+        all_neg = all_neg && idx[k] < 0;
+      }
+      if (all_zero || all_neg) s_bad = 1;
+    }
+    __syncthreads();
+    if (s_bad) {
+      if (tid == 0) {
+        valid[sample] = 0;
+        eloc[sample] = 0.0;
+        lpsi[sample] = 0.0;
+      }
+      for (int k = tid; k < m.sr_size; k += nt) orow[k] = 0.0;
+      __syncthreads();
+      continue;
+    }
+    for (int q = 0; q < m.nqp; ++q) {
+      for (int i = warp; i < n - 1; i += nwarp) {  // X(i, j), i < j, from the Slater table
+        const int ri = idx[i] + (i >= ne ? ns : 0);
+        const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + ri) * m.ns2;
+        for (int j = i + 1 + lane; j < n; j += 32) P[rs[i] + j] = __ldg(srow + idx[j] + (j >= ne ? ns : 0));
+      }
+      __syncthreads();
+      double pfv;
+      int st;
+      gj_pfinv_packed<JPL, (kPackedThreads > 512 ? 1 : 2)>(P, rs, n, rowp, rowq, pfv, st);
+      if (st != 0) {
+        if (tid == 0) s_bad = 1;
+        __syncthreads();
+        break;
+      }
+      if (tid == 0) pf[q] = pfv;
+      const double wq = m.qpw[q];
+      // transfer terms: one-electron ratio on this plane (warp per term)
+      for (int t = warp; t < m.nterm; t += nwarp) {
+        const int ti = m.tterm[4 * t], tsi = m.tterm[4 * t + 1], tj = m.tterm[4 * t + 2], tsj = m.tterm[4 * t + 3];
+        const int dst = ti + tsi * ns, src = tj + tsj * ns;
+        if (tsi != tsj || (ti == tj) || num[dst] == 1 || num[src] == 0 || cfg[src] < 0) continue;
+        const int msj = cfg[src] + tsj * ne;
+        const int rsa = ti + tsj * ns;
+        const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + rsa) * m.ns2;
+        double sv[JPL];  // the gathered Slater row: every load of the lane in flight at once
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int k = lane + 32 * c;
+          sv[c] = k < n ? __ldg(srow + (k == msj ? ti : idx[k]) + (k >= ne ? ns : 0)) : 0.0;
+        }
+        double r = 0.0;
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int k = lane + 32 * c;
+          if (k < n) r += packed_at(P, rs, msj, k) * sv[c];
+        }
+        r = warp_sum(r);
+        if (lane == 0) {
+          const double v = wq * (-r * pfv);
+          if (q == 0) tacc[t] = v;  // a plain store: no read of the block's workspace
+          else tacc[t] += v;
+        }
+      }
+      // Slater derivative by orbital: electron pairs (i, j) on the orbital's site pairs
+      const int trans = q / m.nleg, spidx = q % m.nleg, mpidx = trans % m.nmp;
+      for (int k = tid; k < ns; k += nt) {
+        const int a = m.trans_inv[mpidx * ns + k];
+        tinv[k] = a;
+        tsg[a] = m.trans_sgn[mpidx * ns + a];
+      }
+      __syncthreads();
+      const double cs = pfv * m.spgl[spidx], cc = pfv * m.spgl[m.nleg + spidx], ss = pfv * m.spgl[2 * m.nleg + spidx];
+      const double fac[4] = {cs, -cc, ss, -cs};  // (up, up), (up, dn), (dn, up), (dn, dn)
+      for (int k = tid; k < m.norb; k += nt) {
+        double acc = 0.0;
+        const int e1 = __ldg(m.orb_off + k + 1);
+        for (int e = __ldg(m.orb_off + k); e < e1; ++e) {
+          const int ent = __ldg(m.orb_ent + e);
+          const int a = tinv[ent >> 16], b = tinv[(ent >> 1) & 0x7fff];
+          const int sgn = (ent & 1 ? -1 : 1) * tsg[a] * tsg[b];
+#pragma unroll
+          for (int sa = 0; sa < 2; ++sa) {
+            const int ei = cfg[a + sa * ns];
+            if (ei < 0) continue;
+#pragma unroll
+            for (int sb = 0; sb < 2; ++sb) {
+              const int ej = cfg[b + sb * ns];
+              if (ej < 0) continue;
+              const double v = packed_at(P, rs, ei + sa * ne, ej + sb * ne);
+              acc += (fac[2 * sa + sb] * v) * static_cast<double>(sgn);
+            }
+          }
+        }
+        orow[1 + m.nproj + k] += wq * acc;
+      }
+      __syncthreads();
+    }
+    if (s_bad) {
+      if (tid == 0) {
+        valid[sample] = 0;
+        eloc[sample] = 0.0;
+        lpsi[sample] = 0.0;
+        atomicOr(status, kDevSingular);
+      }
+      for (int k = tid; k < m.sr_size; k += nt) orow[k] = 0.0;
+      __syncthreads();
+      continue;
+    }
+    double ip = 0.0;
+    for (int q = 0; q < m.nqp; ++q) ip += m.qpw[q] * pf[q];
+    for (int t = tid; t < m.nterm; t += nt) {
+      const int ti = m.tterm[4 * t], tsi = m.tterm[4 * t + 1], tj = m.tterm[4 * t + 2], tsj = m.tterm[4 * t + 3];
+      const int dst = ti + tsi * ns, src = tj + tsj * ns;
+      double g;
+      if (tsi == tsj && ti == tj) g = static_cast<double>(num[src]);
+      else if (tsi != tsj || num[dst] == 1 || num[src] == 0 || cfg[src] < 0) g = 0.0;
+      else g = exp(direct_hop_log_proj(m, num, cj, tj, ti, src, dst)) * tacc[t] / ip;
+      // the transfer sum Σ_t −t_t·g_t in a fixed order: per thread over its terms, warps
+      // by shuffles, warps in order below
+      g1[t] = -m.tval[t] * g;
+    }
+    double part = 0.0;
+    for (int t = tid; t < m.nterm; t += nt) part += g1[t];
+    part = warp_sum(part);
+    if (lane == 0) rowq[warp] = part;  // the sweep's row buffer is free here
+    __syncthreads();
+    if (tid == 0) {
+      double e = 0.0;
+      for (int k = 0; k < m.nintra; ++k) {
+        const int i = m.intra_i[k];
+        e += m.intra_v[k] * static_cast<double>(num[i] * num[i + ns]);
+      }
+      for (int k = 0; k < m.ninter; ++k) {
+        const int i = m.inter_ij[2 * k], j = m.inter_ij[2 * k + 1];
+        e += m.inter_v[k] * static_cast<double>(num[i] + num[i + ns]) * static_cast<double>(num[j] + num[j + ns]);
+      }
+      for (int k = 0; k < m.nhund; ++k) {
+        const int i = m.hund_ij[2 * k], j = m.hund_ij[2 * k + 1];
+        e -= m.hund_v[k] * (static_cast<double>(num[i] * num[j]) + static_cast<double>(num[i + ns] * num[j + ns]));
+      }
+      double transfer = 0.0;
+      for (int w = 0; w < nwarp; ++w) transfer += rowq[w];
+      e += transfer;
+      const bool ok = fabs(ip) >= 1.0e-100 && isfinite(e);
+      valid[sample] = ok ? 1 : 0;
+      eloc[sample] = ok ? e : 0.0;
+      double lp = 0.0;
+      for (int k = 0; k < m.nproj; ++k) lp += m.proj[k] * static_cast<double>(cnt[k]);
+      lpsi[sample] = ok ? lp + log(fabs(ip)) : 0.0;
+      pf[m.nqp + 1] = ok ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const bool ok = pf[m.nqp + 1] != 0.0;
+    const double inv_ip = ip / (ip * ip);
+    for (int k = tid; k < m.sr_size; k += nt) {
+      double v;
+      if (k == 0) v = 1.0;
+      else if (k <= m.nproj) v = static_cast<double>(cnt[k - 1]);
+      else v = orow[k] * inv_ip;
+      orow[k] = ok ? v : 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+bool packed_measure_fits(const DevModel& m, int limit) {
+  return m.orb_off != nullptr && m.trans_inv != nullptr && m.n <= 256 &&
+         packed_layout(m).total <= static_cast<size_t>(limit);
+}
+
+template <int JPL>
+int launch_measure_packed(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num, const int* s_cnt,
+                          int nsamples, double* gws, size_t gws_stride, int gws_blocks, double* ostore, double* eloc,
+                          double* lpsi, int* valid, unsigned* status, cudaStream_t stream) {
+  const size_t smem = packed_layout(m).total;
+  auto kernel = k_measure_packed<JPL>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const int grid = std::max(1, std::min({nsamples, gws_blocks, current_device_attr(cudaDevAttrMultiProcessorCount)}));
+  kernel<<<grid, kPackedThreads, smem, stream>>>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_stride, ostore,
+                                                 eloc, lpsi, valid, status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
 }
 
 // Per-walker sums in sample order: [Wc, E, E², Sz, Sz²] and HO, ⟨O⟩, ⟨O²⟩ (unnormalised).
@@ -710,17 +1003,11 @@ int launch_measure_jpl(const DevModel& m, const int* s_idx, const int* s_cfg, co
                                          lpsi, valid, gval, status, stream, limit);
 }
 
-bool cluster_measure_fits(const DevModel& m, int limit);
-int launch_measure_cluster(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
-                           const int* s_cnt, int nsamples, double* scratch, size_t scratch_len, double* ostore,
-                           double* eloc, double* lpsi, int* valid, unsigned* status, int limit, cudaStream_t stream);
 
 // gval != nullptr selects the PhysCal form: Green rows [nsamples][m.gw] instead of O rows.
-// Planes that do not fit one SM's shared memory are swept by one CTA per sample in its
-// L2 workspace; MVMC_B200_MEASURE=cluster measures them with two-CTA clusters holding half
-// the rows each in shared memory (measure_cluster.cu), which measured 1.8× slower at
-// n = 224 (72.8 vs 40.2 ms for 2048 samples: two cluster barriers and two remote row reads
-// per pivot step).
+// Planes that do not fit one SM's shared memory are swept as packed upper triangles in
+// shared memory (k_measure_packed) when those fit, else in place in each block's L2
+// workspace (MVMC_B200_MEASURE=l2 selects the latter).
 int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const int* s_num,
                    const int* s_cnt, int nsamples, double* gws, int gws_blocks, double* ostore,
                    double* eloc, double* lpsi, int* valid, double* gval, unsigned* status, cudaStream_t stream) {
@@ -728,12 +1015,17 @@ int launch_measure(const DevModel& m, const int* s_idx, const int* s_cfg, const 
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int n = m.n;
-  if (!gval && meas_layout(m, true).total > static_cast<size_t>(limit) && cluster_measure_fits(m, limit)) {
-    const char* e = std::getenv("MVMC_B200_MEASURE");
-    if (e && std::strcmp(e, "cluster") == 0)
-      return launch_measure_cluster(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws,
-                                    static_cast<size_t>(gws_blocks) * 2 * n * n, ostore, eloc, lpsi, valid, status,
-                                    limit, stream);
+  const char* mode = std::getenv("MVMC_B200_MEASURE");
+  // planes too large for shared memory whose upper triangle fits: the packed sweep
+  // (MVMC_B200_MEASURE=l2 keeps the in-place sweep of full planes in L2)
+  const size_t gws_stride = static_cast<size_t>(2) * n * n;
+  if (!gval && meas_layout(m, true).total > static_cast<size_t>(limit) && packed_measure_fits(m, limit) &&
+      gws_stride >= static_cast<size_t>(2) * m.nterm && !(mode && std::strcmp(mode, "l2") == 0)) {
+    if (n <= 224)
+      return launch_measure_packed<7>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_stride, gws_blocks, ostore,
+                                      eloc, lpsi, valid, status, stream);
+    return launch_measure_packed<8>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_stride, gws_blocks, ostore,
+                                    eloc, lpsi, valid, status, stream);
   }
 #define MVMCB_MEASURE(J) \
   launch_measure_jpl<J>(m, s_idx, s_cfg, s_num, s_cnt, nsamples, gws, gws_blocks, ostore, eloc, lpsi, valid, gval, \

@@ -401,3 +401,155 @@ __device__ void gj_pfinv_pp(T* A, T* B, int n, double& pf_out, int& status_out) 
 }
 
 }  // namespace mvmcb
+
+namespace mvmcb {
+
+// Packed form of the sweep for planes whose full n×n FP64 matrix exceeds shared memory but
+// whose strict upper triangle fits (n = 224: 195 KB): A(i, j), i < j, lives at
+// P[rs[i] + j] with rs[i] = i·n − i(i+1)/2 − i − 1; A(j, i) = −A(i, j) and A(i, i) = 0, and
+// the sweep keeps the matrix skew, so updating the triangle suffices (half the flops and
+// bytes of the full sweep). Same pivot rule and status codes as gj_pfinv_pp; the element
+// update A(i, j) += (A(q, i)/a)·A(p, j) − (A(p, i)/a)·A(q, j) scales the row coefficients
+// first (two dependent FMAs per element). Per pivot step: every warp finds (p, q) redundantly from the snapshot of row
+// p, the CTA snapshots row q (one barrier), then updates the triangle in place, writing
+// the snapshot of the next pivot row as it goes (one barrier). rowp is [2][n] (double
+// buffered), rowq [n]; on exit P holds the triangle of X⁻¹.
+__device__ __forceinline__ double packed_at(const double* P, const int* rs, int i, int j) {
+  return i < j ? P[rs[i] + j] : (i > j ? -P[rs[j] + i] : 0.0);
+}
+
+template <int JPL, int RB = 2>
+__device__ void gj_pfinv_packed(double* P, const int* rs, int n, double* rowp2, double* rowq, double& pf_out,
+                                int& status_out) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  unsigned swept = 0;  // bit c: column lane + 32c swept (identical in every warp)
+  int p = 0, parity = 0, status = 0;
+  double pf = 1.0;
+  double* rowp = rowp2;
+  for (int j = tid; j < n; j += nt) rowp[j] = packed_at(P, rs, 0, j);
+  __syncthreads();
+  for (int k = 0; k < n / 2; ++k) {
+    // pivot q of row p: first maximum of |A(p, j)| over unswept j ≠ p (every warp)
+    double best = -1.0;
+    int bi = n;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j < n && j != p && !((swept >> c) & 1u)) {
+        const double v = fabs(rowp[j]);
+        if (v > best) {
+          best = v;
+          bi = j;
+        }
+      }
+    }
+    warp_argmax_first(best, bi);
+    const int q = __shfl_sync(0xffffffffu, bi, 0);
+    best = __shfl_sync(0xffffffffu, best, 0);
+    if (!(best > 0.0)) {
+      status = p + 1;
+      break;  // every warp read the same snapshot: all leave together
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      cnt += (j < n && !((swept >> c) & 1u) && j > p && j < q) ? 1 : 0;
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    parity += cnt;
+    const double a = rowp[q];
+    pf *= a;
+    const double ia = 1.0 / a;
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j == p || j == q) swept |= 1u << c;
+    }
+    int pn = n;  // next pivot row: smallest unswept index
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      if (j < n && !((swept >> c) & 1u) && j < pn) pn = j;
+    }
+    for (int off = 16; off > 0; off >>= 1) pn = min(pn, __shfl_xor_sync(0xffffffffu, pn, off));
+    for (int j = tid; j < n; j += nt) rowq[j] = packed_at(P, rs, q, j);
+    __syncthreads();
+    double* rown = rowp == rowp2 ? rowp2 + n : rowp2;  // snapshot of the next pivot row
+    if (tid == 0 && pn < n) rown[pn] = 0.0;
+    // lane l owns columns j = l + 32c: the pivot rows' values of its columns stay in
+    // registers for the whole step, and two rows' loads are issued before any store. Rows
+    // p and q are rewritten by warps 0 and 1 after the others; in the other rows the
+    // columns p, q and pn are single slots (c, lane) known before the loop, and chunks of
+    // 32 columns that lie wholly left of the diagonal are skipped.
+    double rp[JPL], rq[JPL];
+#pragma unroll
+    for (int c = 0; c < JPL; ++c) {
+      const int j = lane + 32 * c;
+      rp[c] = j < n ? rowp[j] : 0.0;
+      rq[c] = j < n ? rowq[j] : 0.0;
+    }
+    const int cp_ = lane == (p & 31) ? p >> 5 : -1, cq_ = lane == (q & 31) ? q >> 5 : -1;
+    const int cn_ = pn < n && lane == (pn & 31) ? pn >> 5 : -1;
+    for (int i0 = warp; i0 < n - 1; i0 += nwarp * RB) {
+      double x[RB][JPL];
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        const bool row_on = i < n - 1 && i != p && i != q;
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          x[r][c] = (row_on && 32 * c + 31 > i && j > i && j < n) ? P[rs[i] + j] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r * nwarp;
+        if (i >= n - 1 || i == p || i == q) continue;
+        // the row's coefficients scaled by 1/a first: two dependent FMAs per element
+        const double ai = rowq[i] * ia, bi = rowp[i] * ia;
+        double* Pi = P + rs[i];
+        const bool is_pn = i == pn;
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          if (32 * c + 31 <= i) continue;  // wholly left of the diagonal (uniform)
+          const int j = lane + 32 * c;
+          if (j <= i || j >= n) continue;
+          double v = x[r][c] + ai * rp[c] - bi * rq[c];
+          if (c == cp_) v = -ai;  // column p
+          if (c == cq_) v = bi;   // column q
+          Pi[j] = v;
+          if (is_pn) rown[j] = v;
+          if (c == cn_) rown[i] = -v;  // column of the next pivot row
+        }
+      }
+    }
+    if (warp == 0 || warp == (1 % nwarp)) {  // rows p (warp 0) and q (warp 1)
+      for (int which = (warp == 0 ? 0 : 1); which < 2; which += (nwarp > 1 ? 2 : 1)) {
+        const int i = which == 0 ? p : q;
+        double* Pi = P + rs[i];
+#pragma unroll
+        for (int c = 0; c < JPL; ++c) {
+          const int j = lane + 32 * c;
+          if (j <= i || j >= n) continue;
+          const double v = which == 0 ? (j == q ? -ia : rq[c] * ia) : -rp[c] * ia;
+          Pi[j] = v;
+          if (c == cn_) rown[i] = -v;
+        }
+      }
+    }
+    p = pn < n ? pn : 0;
+    rowp = rown;
+    __syncthreads();
+  }
+  double v = (parity & 1) ? -pf : pf;
+  if (status == 0 && !isfinite(v)) status = -1;
+  if (status != 0) v = 0.0;
+  pf_out = v;
+  status_out = status;
+  __syncthreads();
+}
+
+}  // namespace mvmcb

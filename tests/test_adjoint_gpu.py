@@ -25,8 +25,12 @@ def inputs(tmp_path, name, interval, **over):
     return lat.write_inputs(str(tmp_path / name), **cfg)
 
 
-@pytest.mark.parametrize("name,over", [("square8", {}), ("square8", {"tp": -0.2, "n_up": 28})])
+@pytest.mark.parametrize("name,over", [("square8", {}), ("square8", {"tp": -0.2, "n_up": 28}), ("square16", {})])
 def test_o_rows_match_central_differences(tmp_path, name, over):
+    """64 random (sample, parameter) pairs per model: 2D 8x8 at half filling, 2D 8x8 with
+    t' = -0.2 at 56 electrons, and the 2D 16x16 adjoint-check model (t' = -0.2, U = 6,
+    112 + 112 electrons, n = 224, full translation symmetry: inverse planes swept as packed
+    triangles in shared memory)."""
     nl, init, dims = inputs(tmp_path, name, 2, **over)
     W = 32
     eng = mvmc().Engine(nl, init, walkers=W, precision=64, seed=5)
@@ -67,12 +71,15 @@ def test_o_rows_match_central_differences(tmp_path, name, over):
     eng.close()
 
 
-@pytest.mark.parametrize("measure", ["single", "cluster"])
+@pytest.mark.parametrize("measure", ["packed", "l2"])
 def test_o_rows_match_oracle_sroopt_on_32_walkers(tmp_path, monkeypatch, measure):
-    """2D 16x16 (t' = -0.2, 112 + 112 electrons, n = 224, inverse planes in L2): every
-    configuration of the 32 chains equals the oracle's, and so do the SROptO rows — with
-    the measurement on one CTA per sample and on two-CTA clusters."""
-    monkeypatch.setenv("MVMC_B200_MEASURE", measure)
+    """2D 16x16 (t' = -0.2, 112 + 112 electrons, n = 224): every configuration of the 32
+    chains equals the oracle's, and so do the SROptO rows — with the planes swept as packed
+    triangles in shared memory (default) and in place in L2."""
+    if measure == "l2":
+        monkeypatch.setenv("MVMC_B200_MEASURE", "l2")
+    else:
+        monkeypatch.delenv("MVMC_B200_MEASURE", raising=False)
     nl, init, dims = inputs(tmp_path, "square16", 1)
     W = 32
     _, ref = ol.opt_step1_walkers(nl, W, seed=21, initial_def=init)
@@ -85,4 +92,21 @@ def test_o_rows_match_oracle_sroopt_on_32_walkers(tmp_path, monkeypatch, measure
     o = eng.o_store()
     assert np.allclose(o, ref["ostore"], rtol=1e-10, atol=1e-11 * np.abs(ref["ostore"]).max())
     assert np.allclose(ho, ref["ho"], rtol=1e-10, atol=1e-11 * np.abs(ref["ho"]).max())
+    eng.close()
+
+
+@pytest.mark.parametrize("name", ["square8", "square16"])
+def test_o_rows_are_bitwise_repeatable(tmp_path, name):
+    """The same saved samples measured twice give bit-identical O rows, energies and sums:
+    every reduction, the Slater derivative included, runs in a fixed order (2D 8x8 with 8
+    QP planes in shared memory; 2D 16x16, n = 224, packed triangles)."""
+    nl, init, dims = inputs(tmp_path, name, 1)
+    eng = mvmc().Engine(nl, init, walkers=64, precision=64, seed=3)
+    eng.sample()
+    e1, ho1, oo1 = eng.measure()
+    o1 = eng.o_store().copy()
+    e2, ho2, oo2 = eng.measure()
+    o2 = eng.o_store()
+    assert np.array_equal(o1, o2)
+    assert np.array_equal(e1, e2) and np.array_equal(ho1, ho2) and np.array_equal(oo1, oo2)
     eng.close()

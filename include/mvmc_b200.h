@@ -63,6 +63,14 @@ int mvmc_b200_pfinv_batch_complex(const double* x, int n, int planes, double* pf
 int mvmc_b200_pfinv_batch_complex_device(const double* x, int n, int planes, double* pf, double* inv,
                                          int* status, void* stream);
 
+/* Gram matrix on the tensor cores (the Oᵀ·O of the SR matrix, SrStages::gram_real,
+ * crates/mvmc-core/src/sr_backend.rs:464; the reference GPU path's cuBLAS dgemm,
+ * gpu/mvmc-gpu-cuda/src/opt.rs:1133-1147): gram[na][na] (host, FP32) = Σ_s x_s x_sᵀ of
+ * samples[ns][na] (host, row-major), the samples rounded to BF16 (precision 16) or read as
+ * TF32 (precision 32), FP32 accumulation (tcgen05.mma). Returns 1 when a bounded device
+ * wait expired (no result), < 0 on errors. Allocates device memory. */
+int mvmc_b200_gram_tc(const double* samples, long long ns, int na, int precision, float* gram);
+
 /* ---------------------------------------------------------------------------------
  * Walker ensemble engine.
  * ------------------------------------------------------------------------------- */

@@ -28,6 +28,7 @@ EXPORTS = [
     "mvmc_b200_measure_sums", "mvmc_b200_sr_gather", "mvmc_b200_sr_local_product", "mvmc_b200_sr_apply",
     "mvmc_b200_sr_config", "mvmc_b200_physcal_create", "mvmc_b200_green_dims", "mvmc_b200_measure_green",
     "mvmc_b200_run_physcal", "mvmc_b200_pfinv_batch_complex", "mvmc_b200_pfinv_batch_complex_device",
+    "mvmc_b200_gram_tc",
 ]
 
 
@@ -126,6 +127,18 @@ def gram(store):
     samples, n = store.shape
     out = np.zeros((n, n))
     _check(lib().mvmc_b200_gram(_ptr(store), n, ctypes.c_longlong(samples), _ptr(out)), "gram")
+    return out
+
+
+def gram_tc(samples, precision=16):
+    """Σ_s x_s x_sᵀ (FP32) of samples [ns, na] on the tensor cores: BF16 (16) or TF32 (32)
+    inputs, FP32 accumulation. Raises when a bounded device wait expired."""
+    samples = np.ascontiguousarray(samples, dtype=np.float64)
+    ns, na = samples.shape
+    out = np.zeros((na, na), dtype=np.float32)
+    rc = _check(lib().mvmc_b200_gram_tc(_ptr(samples), ctypes.c_longlong(ns), na, precision, _ptr(out)), "gram_tc")
+    if rc != 0:
+        raise RuntimeError("gram_tc: a bounded device wait expired")
     return out
 
 

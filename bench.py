@@ -355,9 +355,10 @@ def sr16_record(args, local, timed=3):
     """The 2D 16×16 SR workload (t' = -0.2, U = 6, 112 + 112 electrons, n = 224, 4×4-sublattice
     f: 4226 parameters, 8192 walkers, SR-CG): SR-step time split into sampling, measurement
     and SR-CG for the plain FP64 path and the mixed path (FP32 inverse updates with FP64
-    refresh, BF16 centred column-scaled SR operator), and the mixed path's errors on the first
-    step from the same seeds and parameters: energy per site, variance, <O_k> and the SR
-    parameter update; the update error of the BF16 operator alone on the FP64 path's samples."""
+    refresh; SR-CG through the tensor-core Gram of the centred, column-scaled samples with
+    TF32 inputs), and the mixed path's errors on the first step from the same seeds and
+    parameters: energy per site, variance, <O_k> and the SR parameter update; the update
+    error of each reduced-precision SR operator alone on the FP64 path's samples."""
     import torch
     import lattice
     import mvmc_b200 as mb
@@ -366,17 +367,18 @@ def sr16_record(args, local, timed=3):
     nl, init, dims = lattice.write_inputs(os.path.join(tmp, "in"), **cfg)
     W = WALKERS["square16_sr"]
 
-    def run(precision, sr_precision, steps):
+    def run(precision, sr_precision, steps, sr_gram=0):
         eng = mb.Engine(nl, init, walkers=W, precision=precision, seed=12345,
                         refresh_sweeps=args.refresh if precision == 32 else 0,
-                        refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision)
+                        refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision,
+                        sr_gram=sr_gram)
         stream = torch.cuda.ExternalStream(eng.stream())
         p0 = eng.parameters()
         eng.sample()
         e, ho, oo = eng.measure()
         idx = eng.samples()["ele_idx"].reshape(W, -1)
-        eng.sr_cg()
-        first = {"e": e, "oo": oo, "dp": eng.parameters() - p0, "idx": idx}
+        _, info = eng.sr_cg()
+        first = {"e": e, "oo": oo, "dp": eng.parameters() - p0, "idx": idx, "cg_info": int(info[8])}
         if steps == 0:
             eng.close()
             return first, None
@@ -399,8 +401,11 @@ def sr16_record(args, local, timed=3):
                        "sr_step_ms": float(s.sum())}
 
     a_first, a_t = run(64, 64, timed)
-    c_first, c_t = run(32, 16, timed)
-    b_first, _ = run(64, 16, 0)
+    c_first, c_t = run(32, 32, timed, sr_gram=1)
+    op_err = {}
+    for name, srp, gram in (("tf32_gram", 32, 1), ("bf16_gram", 16, 1), ("bf16_gemv", 16, 0)):
+        f, _ = run(64, srp, 0, sr_gram=gram)
+        op_err[name] = float(np.linalg.norm(f["dp"] - a_first["dp"]) / max(np.linalg.norm(a_first["dp"]), 1e-300))
     ns = dims["nsite"]
     size = 1 + dims["npara"]
     var = lambda f: float(f["e"][2] - f["e"][1] ** 2)
@@ -414,14 +419,17 @@ def sr16_record(args, local, timed=3):
                             "measure": a_t["measure_ms"] / c_t["measure_ms"],
                             "sr_cg": a_t["sr_cg_ms"] / c_t["sr_cg_ms"]},
         "mixed_precision": {"sampler": "f32 updates + f64 refresh", "refresh_sweeps": args.refresh,
-                            "refresh_guard": args.guard, "sr_operator": "bf16 centred, column-scaled"},
+                            "refresh_guard": args.guard,
+                            "sr_operator": "Gram of the centred, column-scaled samples on the tensor cores "
+                                           "(tcgen05, TF32 inputs, FP32 accumulation), FP64 CG"},
+        "cg_status_first_step": {"fp64": a_first["cg_info"], "mixed": c_first["cg_info"]},
         "accuracy_first_step": {
             "identical_chains": float(np.mean(np.all(a_first["idx"] == c_first["idx"], axis=1))),
             "dE_per_site": float(abs(c_first["e"][1] - a_first["e"][1]) / ns),
             "variance_fp64": var(a_first), "dvariance": abs(var(c_first) - var(a_first)),
             "max_dO_mean": float(np.max(np.abs(c_first["oo"][:size] - a_first["oo"][:size]))),
             "update_rel_err_mixed": rel(c_first["dp"], a_first["dp"]),
-            "update_rel_err_bf16_operator_only": rel(b_first["dp"], a_first["dp"])},
+            "update_rel_err_operator_only": op_err},
     }
 
 

@@ -91,6 +91,10 @@ typedef struct mvmc_b200_options {
                          * order without FMA (pfapack LTLᵀ inverse, serial sums; results equal the
                          * CPU path's bit for bit up to libm's exp): the parity mode of the 10-step
                          * zvo_out.dat gate (phase5_zvo_gate_hubbard.rs:19-80). 0: throughput kernels. */
+  int sr_gram;          /* 1 with sr_precision 16 / 32: SR-CG applies S through the Gram G = OᵀO of the
+                         * centred, column-scaled samples, formed once per SR step on the tensor cores
+                         * (BF16 / TF32 inputs, FP32 accumulation); 0: one pass over the samples per
+                         * CG product */
 } mvmc_b200_options;
 
 void mvmc_b200_default_options(mvmc_b200_options* opt);

@@ -26,6 +26,7 @@ enum DeviceStatus : unsigned {
   kDevInitLoops = 4u,      // makeInitialSample exhausted its retries
   kDevBounds = 8u,         // an index check failed (checked builds)
   kDevCandidateLoop = 16u, // a proposal loop exceeded its bound
+  kDevTimeout = 32u,       // a bounded device wait (mbarrier) expired
 };
 
 #define MVMCB_CUDA(call)                                                         \

@@ -35,6 +35,11 @@ int launch_measure_corder(const DevModel& m, int W, int S, const int* s_idx, con
                           const int* s_cnt, double* ostore, double* eloc, double* lpsi, int* valid, double* wsum,
                           double* dscr, int* iscr, cudaStream_t stream);
 int launch_cg_corder(const CgArgs& a, int W, int S, cudaStream_t stream);
+void gram_tc_dims(int na, long long ns, int precision, int* na_pad, long long* ld);
+int launch_gram_stage(const double* store, int sr_size, long long ns, const int* map, int na, const double* mean,
+                      const double* cs, int precision, void* staged, cudaStream_t stream);
+int launch_gram_tc(const void* staged, int na, long long ns, int precision, float* G, int ldg, unsigned* status,
+                   cudaStream_t stream);
 int launch_gather_active(const double* store, int sr_size, long long ns, const int* map, int na,
                          double* oa, cudaStream_t stream);
 int launch_sr_cg(CgArgs a, cudaStream_t stream);
@@ -123,6 +128,10 @@ struct mvmc_b200_ctx {
   double* d_tot = nullptr;
   double* d_gws = nullptr;
   double* d_cscr = nullptr;  // C-order measurement scratch (per walker), allocated on first use
+  void* d_staged = nullptr;  // Gram form: centred, column-scaled, transposed active samples
+  size_t staged_cap = 0;
+  float* d_gram = nullptr;   // Gram form: G = OᵀO (FP32, na × na)
+  size_t gram_cap = 0;
   int* d_cscr_i = nullptr;
   int gws_blocks = 0;
   // SR-CG buffers
@@ -780,9 +789,32 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   }
   check(cudaMemcpyAsync(c->d_cgvec, vecs.data(), sizeof(double) * 3 * na, cudaMemcpyHostToDevice, c->stream),
         "upload cg vectors");
-  int rc = kind == 0 ? launch_gather_active(c->d_ostore, size, ns, c->d_map, na, c->d_oa, c->stream)
-                     : launch_gather_active_low(c->d_ostore, size, ns, c->d_map, na, c->d_cgvec,
-                                                c->d_cgvec + 7 * static_cast<size_t>(na), kind, c->d_oa, c->stream);
+  // Gram form: G = OlᵀOl on the tensor cores (BF16 for sr_precision 16, TF32 for 32)
+  const bool gram = kind != 0 && c->opt.sr_gram != 0;
+  int rc;
+  if (gram) {
+    const int prec = kind == 2 ? 16 : 32;
+    int na_pad = 0;
+    long long ld = 0;
+    gram_tc_dims(na, ns, prec, &na_pad, &ld);
+    const size_t staged = static_cast<size_t>(na_pad) * ld * (prec == 16 ? 2 : 4);
+    if (staged > c->staged_cap) {
+      c->d_staged = c->alloc<unsigned char>(staged);
+      c->staged_cap = staged;
+    }
+    if (static_cast<size_t>(na) * na > c->gram_cap) {
+      c->d_gram = c->alloc<float>(static_cast<size_t>(na) * na);
+      c->gram_cap = static_cast<size_t>(na) * na;
+    }
+    rc = launch_gram_stage(c->d_ostore, size, ns, c->d_map, na, c->d_cgvec, c->d_cgvec + 7 * static_cast<size_t>(na),
+                           prec, c->d_staged, c->stream);
+    if (rc != kOk) return rc;
+    rc = launch_gram_tc(c->d_staged, na, ns, prec, c->d_gram, na, c->dw.status, c->stream);
+  } else {
+    rc = kind == 0 ? launch_gather_active(c->d_ostore, size, ns, c->d_map, na, c->d_oa, c->stream)
+                   : launch_gather_active_low(c->d_ostore, size, ns, c->d_map, na, c->d_cgvec,
+                                              c->d_cgvec + 7 * static_cast<size_t>(na), kind, c->d_oa, c->stream);
+  }
   if (rc != kOk) return rc;
   CgArgs a;
   a.O = c->d_oa;
@@ -806,10 +838,10 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   a.shift = m.sta_del;
   a.tol = m.cg_tol;
   if (kind != 0) {
-    a.Ol = c->d_oa;
+    a.Ol = gram ? static_cast<const void*>(c->d_gram) : static_cast<const void*>(c->d_oa);
     a.cs = c->d_cgvec + 7 * static_cast<size_t>(na);
-    a.lda = low_lda(na, kind);
-    a.o_kind = kind;
+    a.lda = gram ? na : low_lda(na, kind);
+    a.o_kind = gram ? 3 : kind;
   }
   auto solve = [&]() { return c->opt.c_order ? launch_cg_corder(a, c->W, c->S, c->stream) : launch_sr_cg(a, c->stream); };
   rc = solve();
@@ -820,6 +852,11 @@ int do_sr_cg(mvmc_b200_ctx* c, double* info_out) {
   check(cudaStreamSynchronize(c->stream), "sr-cg");
   c->h2d += static_cast<long long>(sizeof(int) * na + sizeof(double) * 3 * na);
   c->d2h += static_cast<long long>(sizeof(double) * (na + 8));
+  if (gram) {
+    unsigned dst = 0;
+    check(cudaMemcpy(&dst, c->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+    if (dst & kDevTimeout) throw std::runtime_error("sr-cg: the tensor-core Gram timed out (cuda device wait)");
+  }
   long long status = static_cast<long long>(scal[1]);
   long long info = status;
   if (status < 0) {

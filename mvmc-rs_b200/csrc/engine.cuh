@@ -124,6 +124,8 @@ struct CgArgs {
   // Reduced-precision operator (o_kind 1: FP32, 2: BF16): the centred, column-scaled
   // active matrix Ol[s][i] = (O[s][i] − ⟨O⟩_i)/cs[i] (zero rows for skipped samples), row
   // stride lda, so that S·v = Wc⁻¹·cs ⊙ Olᵀ(Ol·(cs ⊙ v)) + shift·diag ⊙ v. o_kind 0 uses O.
+  // o_kind 3: Ol is the FP32 Gram G = OlᵀOl (na × na, row stride lda) formed on the tensor
+  // cores, so that S·v = Wc⁻¹·cs ⊙ G·(cs ⊙ v) + shift·diag ⊙ v.
   const void* Ol = nullptr;
   const double* cs = nullptr;  // [na]
   int lda = 0;

@@ -35,7 +35,7 @@ namespace mvmcb {
 constexpr int kGramTile = 128;            // M = N = 128 per CTA
 constexpr int kGramStages = 4;            // TMA ring depth
 constexpr int kGramSlabBytes = 128 * 128;  // one operand slab: 128 rows × 128 bytes
-constexpr unsigned kGramTimeout = 1u;      // status bit: a bounded wait expired
+constexpr unsigned kGramTimeout = kDevTimeout;  // status bit: a bounded wait expired
 constexpr long long kGramSpin = 1LL << 26;  // polls before a wait gives up
 
 struct GramSmem {
@@ -392,5 +392,5 @@ extern "C" int mvmc_b200_gram_tc(const double* samples, long long ns, int na, in
   unsigned st = 0;
   MVMCB_CUDA(cudaMemcpy(gram, dg.p, static_cast<size_t>(na) * na * sizeof(float), cudaMemcpyDeviceToHost));
   MVMCB_CUDA(cudaMemcpy(&st, dst.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
-  return st ? 1 : kOk;
+  return (st & kGramTimeout) ? 1 : kOk;
 }

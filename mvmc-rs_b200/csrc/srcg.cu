@@ -18,9 +18,11 @@
 // Reduced-precision operator (mixed path): the active matrix is stored centred and
 // column-scaled in FP32 or BF16 (half or a quarter of the FP64 bytes, so that at the SR
 // configurations it stays in L2 across iterations) and the products accumulate in FP32;
-// vectors, dots and the α/β recurrence stay FP64. The product is a pair of matrix-vector
-// contractions at ≤ 1 flop per byte, bound by memory bandwidth, so it runs on the CUDA
-// cores: tensor cores would add no throughput.
+// vectors, dots and the α/β recurrence stay FP64. As a matrix-vector pair at ≤ 1 flop per
+// byte this form is bound by memory bandwidth on the CUDA cores. The Gram form (o_kind 3)
+// moves the contraction to the tensor cores instead: G = OlᵀOl is formed once per SR step
+// (gram_tc.cu, tcgen05.mma on BF16 or TF32 inputs) and every iteration then applies the
+// L2-resident na × na G, one warp per row.
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -286,6 +288,47 @@ __device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, const
 }
 
 
+// Gram form (o_kind 3): out = Wc⁻¹·cs ⊙ (G·(cs ⊙ v)) + shift·diag ⊙ v with G = ÕᵀÕ formed once
+// on the tensor cores (FP32, na × na, row stride lda). One warp per row of G (FP64
+// accumulation, lanes then shuffles in a fixed order), rows strided over the grid.
+__device__ void sr_apply_gram(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, unsigned char* smem) {
+  double* u = reinterpret_cast<double*>(smem);
+  const int tid = threadIdx.x, nt = blockDim.x, na = a.na, lane = tid & 31;
+  for (int i = tid; i < na; i += nt) u[i] = a.cs[i] * v[i];
+  __syncthreads();
+  const float* G = static_cast<const float*>(a.Ol);
+  const int gw = (blockIdx.x * nt + tid) >> 5, nw = (gridDim.x * nt) >> 5;
+  for (int i = gw; i < na; i += nw) {
+    const float* row = G + static_cast<long long>(i) * a.lda;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    int j = lane;
+    for (; j + 96 < na; j += 128) {
+      t0 += static_cast<double>(__ldg(row + j)) * u[j];
+      t1 += static_cast<double>(__ldg(row + j + 32)) * u[j + 32];
+      t2 += static_cast<double>(__ldg(row + j + 64)) * u[j + 64];
+      t3 += static_cast<double>(__ldg(row + j + 96)) * u[j + 96];
+    }
+    for (; j < na; j += 32) t0 += static_cast<double>(__ldg(row + j)) * u[j];
+    const double t = warp_sum((t0 + t1) + (t2 + t3));
+    if (lane == 0) out[i] = a.inv_w * (a.cs[i] * t) + a.shift * a.diag[i] * v[i];
+  }
+  grid.sync();
+}
+
+struct ApplyGram {
+  unsigned char* smem;
+  __device__ void operator()(cgr::grid_group& g, const CgArgs& a, const double* v, double* out) const {
+    sr_apply_gram(g, a, v, out, smem);
+  }
+};
+
+__global__ void __launch_bounds__(kCgThreads, 1) k_sr_cg_gram(CgArgs a) {
+  cgr::grid_group grid = cgr::this_grid();
+  __shared__ double sh[32 * 8 + 8 + 8];
+  extern __shared__ __align__(16) unsigned char smem[];
+  cg_run(grid, a, sh, ApplyGram{smem});
+}
+
 template <typename OT, int KC>
 __global__ void __launch_bounds__(kCgThreads, 1) k_sr_cg(CgArgs a) {
   cgr::grid_group grid = cgr::this_grid();
@@ -472,6 +515,14 @@ int launch_cg_type(CgArgs& a, cudaStream_t stream) {
 }
 
 int launch_sr_cg(CgArgs a, cudaStream_t stream) {
+  if (a.o_kind == 3) {  // Gram form: G (FP32) in a.Ol, no sample pass per iteration
+    void* args[] = {&a};
+    const size_t smem = sizeof(double) * static_cast<size_t>(a.na);
+    MVMCB_CUDA(cudaFuncSetAttribute(k_sr_cg_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_sr_cg_gram), cg_grid_blocks(a.ns, a.na),
+                                           kCgThreads, args, smem, stream));
+    return kOk;
+  }
   if (a.nchunk < cg_grid_blocks(a.ns, a.na)) {
     set_last_error("sr-cg: partial buffer holds fewer rows than the grid has blocks");
     return kErrArgument;

@@ -96,8 +96,9 @@ def test_guard_reduces_mixed_drift_with_projection(tmp_path):
     assert guarded["drift_max"] * 10 <= plain["drift_max"]
 
 
-def sr_update(nl, init, sr_precision, walkers=1024):
-    eng = mvmc().Engine(nl, init, walkers=walkers, precision=64, seed=7, sr_precision=sr_precision)
+def sr_update(nl, init, sr_precision, walkers=1024, sr_gram=0):
+    eng = mvmc().Engine(nl, init, walkers=walkers, precision=64, seed=7, sr_precision=sr_precision,
+                        sr_gram=sr_gram)
     p0 = eng.parameters()
     eng.sample()
     eng.measure()
@@ -107,13 +108,15 @@ def sr_update(nl, init, sr_precision, walkers=1024):
     return rc, info, dp
 
 
-@pytest.mark.parametrize("sr_precision,bound", [(32, 1e-2), (16, 5e-2)])
-def test_reduced_precision_sr_operator_update_error(tmp_path, sr_precision, bound):
+@pytest.mark.parametrize("sr_precision,sr_gram,bound", [(32, 0, 1e-2), (16, 0, 5e-2), (32, 1, 1e-2), (16, 1, 5e-2)])
+def test_reduced_precision_sr_operator_update_error(tmp_path, sr_precision, sr_gram, bound):
     """The SR parameter update with the FP32 / BF16 centred, column-scaled sample matrix
-    against the FP64 operator on identical samples (same seeds, FP64 sampling)."""
+    (one pass per CG product) and with its Gram formed on the tensor cores (TF32 / BF16
+    inputs, FP32 accumulation) against the FP64 operator on identical samples (same seeds,
+    FP64 sampling)."""
     nl, init, _ = square8_inputs(tmp_path, interval=2)
     rc64, info64, d64 = sr_update(nl, init, 64)
-    rc, info, d = sr_update(nl, init, sr_precision)
+    rc, info, d = sr_update(nl, init, sr_precision, sr_gram=sr_gram)
     assert rc == rc64 == 0
     assert np.array_equal(info[:4], info64[:4]), (info, info64)  # same active set
     assert np.linalg.norm(d64) > 0 and np.linalg.norm(d) > 0, (info, info64)

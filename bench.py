@@ -249,7 +249,10 @@ def time_engine(args, precision, W, namelist, initial_def, cfg, dims, rank, loca
             return t.cpu().numpy()
 
         def sr_step():
-            info = sharded.sr_step(eng, reduce)
+            # CG vectors stay on the GPU: z is added across ranks by an NCCL all-reduce of the
+            # device tensor; the measurement sums go through `reduce` once per step
+            info = sharded.sr_step_device(eng, reduce, dist.all_reduce, "cuda",
+                                          torch.cuda.current_stream().cuda_stream)
             return 0, np.array([info[k] for k in ("npara", "nsmat", "opt_cut", "diag_cut", "sdiag_max",
                                                   "sdiag_min", "rmax", "imax", "info")], dtype=np.float64)
     else:

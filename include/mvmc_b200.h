@@ -292,6 +292,13 @@ int mvmc_b200_sr_gather(mvmc_b200_ctx* ctx, const int* map, int na);
  * context's samples and the gathered columns; no mean, diagonal or cross-rank terms.
  * v, z: na host doubles. */
 int mvmc_b200_sr_local_product(mvmc_b200_ctx* ctx, const double* v, double* z);
+
+/* Device-buffer form of mvmc_b200_sr_local_product (SrStages::cg_local_product on
+ * device-resident vectors, sr_backend.rs:249-255): v and z are device pointers (n_active
+ * doubles) ordered on `stream` (a cudaStream_t); the product is joined to that stream with
+ * events, no host copy is made and nothing is synchronised. A walker-sharded CG then reduces
+ * z across ranks on the device (an NCCL all-reduce of z) without leaving the GPU. */
+int mvmc_b200_sr_local_product_device(mvmc_b200_ctx* ctx, const double* v, double* z, void* stream);
 /* Apply an SR solution: parameter map[i] += x[i], then sync_modified_parameter and the
  * upload (update_parameter_value, sr.rs:439; sync.rs:87). */
 int mvmc_b200_sr_apply(mvmc_b200_ctx* ctx, const int* map, int na, const double* x);

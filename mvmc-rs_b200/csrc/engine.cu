@@ -128,6 +128,7 @@ struct mvmc_b200_ctx {
   double* d_tot = nullptr;
   double* d_gws = nullptr;
   double* d_cscr = nullptr;  // C-order measurement scratch (per walker), allocated on first use
+  cudaEvent_t join_event = nullptr;  // orders device-buffer calls against the caller's stream
   void* d_staged = nullptr;  // Gram form: centred, column-scaled, transposed active samples
   size_t staged_cap = 0;
   float* d_gram = nullptr;   // Gram form: G = OᵀO (FP32, na × na)
@@ -188,6 +189,7 @@ struct mvmc_b200_ctx {
   }
   ~mvmc_b200_ctx() {
     for (void* p : allocs) cudaFree(p);
+    if (join_event) cudaEventDestroy(join_event);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1444,6 +1446,25 @@ extern "C" int mvmc_b200_sr_local_product(mvmc_b200_ctx* c, const double* v, dou
     check(cudaStreamSynchronize(c->stream), "local product");
     c->h2d += static_cast<long long>(sizeof(double) * na);
     c->d2h += static_cast<long long>(sizeof(double) * na);
+    return MVMC_B200_OK;
+  });
+}
+
+// Device-buffer form: v, z are device pointers ordered on the caller's `stream`; the
+// product runs on the engine's stream between two event joins, so no host copy is made.
+extern "C" int mvmc_b200_sr_local_product_device(mvmc_b200_ctx* c, const double* v, double* z, void* stream) {
+  if (!c || !v || !z) return MVMC_B200_EARG;
+  if (c->shard_na <= 0) return MVMC_B200_ESTATE;
+  return guarded([&]() {
+    const long long ns = static_cast<long long>(c->W) * c->S;
+    cudaStream_t caller = static_cast<cudaStream_t>(stream);
+    if (!c->join_event) check(cudaEventCreateWithFlags(&c->join_event, cudaEventDisableTiming), "event");
+    check(cudaEventRecord(c->join_event, caller), "record");
+    check(cudaStreamWaitEvent(c->stream, c->join_event, 0), "join engine stream");
+    const int rc = launch_local_product(c->d_oa, ns, c->shard_na, v, z, c->d_y, c->d_shard_part, c->stream);
+    if (rc != kOk) return rc;
+    check(cudaEventRecord(c->join_event, c->stream), "record");
+    check(cudaStreamWaitEvent(caller, c->join_event, 0), "join caller stream");
     return MVMC_B200_OK;
   });
 }

@@ -145,6 +145,36 @@ __device__ void sr_apply_rows(cgr::grid_group& grid, const CgArgs& a, const doub
   double z[KC];
 #pragma unroll
   for (int k = 0; k < KC; ++k) z[k] = 0.0;
+  if constexpr (R == 1) {
+    // wide rows: four rows per block sum, the rows read twice (their second read hits L1:
+    // 4 rows of at most 8192 FP64 columns), so a product costs a quarter of the barriers
+    constexpr int R2 = 4;
+    for (long long sb = s0; sb < s1; sb += R2) {
+      double y[R2];
+#pragma unroll
+      for (int r = 0; r < R2; ++r) y[r] = 0.0;
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int i = tid + k * nt;
+        if (i >= na) continue;
+        const CT vi = vs[i];
+        CT t[R2];
+#pragma unroll
+        for (int r = 0; r < R2; ++r) t[r] = sb + r < s1 ? Elem<OT>::load(O + (sb + r) * lda + i) : CT(0);
+#pragma unroll
+        for (int r = 0; r < R2; ++r) y[r] += static_cast<double>(t[r] * vi);
+      }
+      block_sum_vec<R2>(y, sh);
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const int i = tid + k * nt;
+        if (i >= na) continue;
+#pragma unroll
+        for (int r = 0; r < R2; ++r)
+          if (sb + r < s1) z[k] += static_cast<double>(Elem<OT>::load(O + (sb + r) * lda + i)) * y[r];
+      }
+    }
+  } else
   for (long long sb = s0; sb < s1; sb += R) {
     CT x[R][KC];
 #pragma unroll

@@ -28,7 +28,7 @@ EXPORTS = [
     "mvmc_b200_measure_sums", "mvmc_b200_sr_gather", "mvmc_b200_sr_local_product", "mvmc_b200_sr_apply",
     "mvmc_b200_sr_config", "mvmc_b200_physcal_create", "mvmc_b200_green_dims", "mvmc_b200_measure_green",
     "mvmc_b200_run_physcal", "mvmc_b200_pfinv_batch_complex", "mvmc_b200_pfinv_batch_complex_device",
-    "mvmc_b200_gram_tc",
+    "mvmc_b200_gram_tc", "mvmc_b200_sr_local_product_device",
 ]
 
 
@@ -271,6 +271,14 @@ class Engine:
         z = np.zeros_like(v)
         _check(lib().mvmc_b200_sr_local_product(self.ctx, _ptr(v), _ptr(z)), "sr_local_product")
         return z
+
+    def sr_local_product_device(self, v, z, stream):
+        """z = Σ_s O_s (O_s·v) on device buffers (CUDA float64 tensors of n_active values, or
+        integer device addresses), ordered on `stream` (an integer cudaStream_t handle)."""
+        vp = ctypes.c_void_p
+        addr = lambda t: t.data_ptr() if hasattr(t, "data_ptr") else int(t)
+        _check(lib().mvmc_b200_sr_local_product_device(self.ctx, vp(addr(v)), vp(addr(z)), vp(stream)),
+               "sr_local_product_device")
 
     def sr_apply(self, mapping, x):
         m = np.ascontiguousarray(mapping, dtype=np.int32)

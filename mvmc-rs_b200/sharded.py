@@ -14,6 +14,12 @@ update, so the parameters stay identical without a broadcast.
 sr_local_product(v) and sr_apply(map, x) — the device Engine of mvmc_b200.py, or a CPU
 stand-in in the tests. `reduce(array) -> array` adds an array across ranks (identity on
 one rank; torch.distributed all_reduce over NCCL in bench.py, gloo in the tests).
+
+sr_step_device keeps the CG vectors in torch tensors on the local product's device: the
+product is `local.sr_local_product_device(v, z, stream)` on device buffers and
+`reduce_(z)` adds z across ranks in place (an NCCL all-reduce of the device tensor), so no
+vector leaves the GPU during the solve; only the recurrence's scalars (the dots that decide
+its branches) are read on the host, as the reference's per-iteration Reducer does.
 """
 import numpy as np
 
@@ -166,6 +172,133 @@ def sr_step(local, reduce):
                 raise RuntimeError("SR-CG failed and fallback is disabled")
             code = -(fallback_iter + 1)
     imax = int(np.argmax(np.abs(x)))  # first maximum, as the C loop
+    info.update(rmax=float(x[imax]), imax=int(mapping[imax]), info=int(code))
+    if not np.all(np.isfinite(x)):
+        if cfg["cg_abort"]:
+            raise RuntimeError("SR-CG produced non-finite updates")
+        return info
+    local.sr_apply(mapping, x)
+    return info
+
+
+def cg_solve_t(apply, g, diag, shift, tol, max_iter, diag_scale):
+    """cg_solve on torch tensors (any device): the same recurrence, statuses and elementwise
+    operation order; dots are tensor sums read on the host for the branch decisions."""
+    import torch
+    n = g.numel()
+    threshold = tol * tol * float(n) * float(n)
+    dq_pre = (1.0 + shift) * diag
+    ok = torch.isfinite(dq_pre) & (dq_pre.abs() >= 1e-12)
+    dq_pre = torch.where(ok, dq_pre, torch.where(dq_pre < 0.0, torch.full_like(dq_pre, -1e-12),
+                                                  torch.full_like(dq_pre, 1e-12)))
+
+    def dot(a, b):
+        return float((a * b).sum())
+
+    x = torch.zeros_like(g)
+    r = g.clone()
+    if diag_scale:
+        r = g - apply(x)
+        d = r / dq_pre
+        delta = dot(r, d)
+    else:
+        d = g.clone()
+        delta = dot(r, r)
+    status, it, done = 0, 0, False
+    if not np.isfinite(delta):
+        return x, -1
+    while it < max_iter:
+        failed = -(it + 1)
+        if not np.isfinite(delta):
+            status, done = failed, True
+            break
+        if abs(delta) < threshold:
+            break
+        q = apply(d)
+        dq = dot(d, q)
+        if not np.isfinite(dq) or abs(dq) < 1e-20:
+            status, done = failed, True
+            break
+        alpha = delta / dq
+        if not np.isfinite(alpha):
+            status, done = failed, True
+            break
+        x = x + alpha * d
+        if (it + 1) % 20 == 0:
+            r = g - apply(x)
+        else:
+            r = r - alpha * q
+        if diag_scale:
+            q = r / dq_pre
+            delta_new = dot(r, q)
+        else:
+            delta_new = dot(r, r)
+        if not np.isfinite(delta_new) or abs(delta) < 1e-20:
+            status, done = failed, True
+            break
+        beta = delta_new / delta
+        if not np.isfinite(beta):
+            status, done = failed, True
+            break
+        if diag_scale:
+            delta = delta_new
+            d = q + beta * d
+        else:
+            delta *= beta
+            d = r + beta * d
+        it += 1
+    if not done:
+        status = -(max_iter + 1) if (it == max_iter and abs(delta) >= threshold) else it
+    return x, status
+
+
+def sr_step_device(local, reduce, reduce_, device, stream=0):
+    """sr_step with the CG vectors on `device` (torch tensors): the local product on device
+    buffers, z added across ranks in place by `reduce_(tensor)`. `reduce` adds the
+    measurement sums (host arrays, once per SR step)."""
+    import torch
+    cfg, flags = local.sr_config()
+    if int(cfg["nsrcg"]) == 0:
+        raise NotImplementedError("the sharded SR step runs SR-CG (NSRCG 1)")
+    npara = int(cfg["npara"])
+    ops = operands(reduce(local.measure_sums()))
+    mapping, var, opt_cut, diag_cut, vmax, vmin = active_set(ops, npara, flags, cfg["red_cut"])
+    info = dict(npara=npara, nsmat=len(mapping), opt_cut=opt_cut, diag_cut=diag_cut, sdiag_max=vmax,
+                sdiag_min=vmin, rmax=0.0, imax=0, info=0)
+    if len(mapping) == 0:
+        return info
+    idx = mapping + 1
+    as_t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
+    mean, diag = as_t(ops["mean"][idx]), as_t(var[mapping])
+    g = as_t(-2.0 * cfg["step_dt"] * (ops["ho"][idx] - ops["ho"][0] * ops["mean"][idx]))
+    inv_w = 1.0 / ops["wc"]
+    shift = cfg["sta_del"]
+    local.sr_gather(mapping)
+
+    def apply(v):
+        v = v.contiguous()
+        z = torch.empty_like(v)
+        local.sr_local_product_device(v, z, stream)
+        reduce_(z)
+        return inv_w * z - (mean * v).sum() * mean + shift * diag * v
+
+    max_iter = int(cfg["cg_max_iter"]) if cfg["cg_max_iter"] > 0 else len(mapping)
+    diag_scale = bool(cfg["diag_scale"])
+    x, status = cg_solve_t(apply, g, diag, shift, cfg["cg_tol"], max_iter, diag_scale)
+    code = status
+    if status < 0:
+        fallback_iter = max(-status - 1, 0)
+        if cfg["cg_fallback"]:
+            x, st2 = cg_solve_t(apply, g, diag, shift, cfg["cg_tol"], max_iter, not diag_scale)
+            code = -(fallback_iter + 1)
+            if st2 < 0 and cfg["cg_abort"]:
+                raise RuntimeError("fallback SR-CG failed")
+        else:
+            if cfg["cg_abort"]:
+                raise RuntimeError("SR-CG failed and fallback is disabled")
+            code = -(fallback_iter + 1)
+    x = x.cpu().numpy()
+    imax = int(np.argmax(np.abs(x)))
     info.update(rmax=float(x[imax]), imax=int(mapping[imax]), info=int(code))
     if not np.all(np.isfinite(x)):
         if cfg["cg_abort"]:

@@ -55,3 +55,25 @@ def test_tf32_gram_matches_fp64_gram_of_tf32_inputs(ns, na):
         errs.append(np.max(np.abs(g - ref) / bound))
     assert min(errs) <= 1.0, errs
     assert np.array_equal(g, g.T)
+
+
+@pytest.mark.parametrize("precision", [16, 32])
+def test_gram_at_the_sr_configuration_shape(precision):
+    """The 2D 16x16 SR configuration's shape (8192 samples × 4226 active parameters): 400
+    random entries against FP64 dot products of the rounded samples (1e-4 relative to
+    Σ|x_i||x_j|), the matrix exactly symmetric."""
+    rng = np.random.default_rng(precision)
+    x = rng.normal(size=(8192, 4226))
+    g = mvmc().gram_tc(x, precision)
+    xr = to_bf16(x) if precision == 16 else None
+    i = rng.integers(0, 4226, 400)
+    j = rng.integers(0, 4226, 400)
+    for a, b in zip(i, j):
+        if precision == 16:
+            ref, scale = xr[:, a] @ xr[:, b], np.abs(xr[:, a]) @ np.abs(xr[:, b])
+        else:
+            cand = [to_tf32(x[:, [a, b]], m) for m in ("trunc", "rn")]
+            ref = min((c[:, 0] @ c[:, 1] for c in cand), key=lambda r: abs(r - g[a, b]))
+            scale = np.abs(x[:, a]) @ np.abs(x[:, b])
+        assert abs(g[a, b] - ref) <= 1e-4 * scale, (a, b, g[a, b], ref)
+    assert np.array_equal(g, g.T)

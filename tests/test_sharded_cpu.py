@@ -43,6 +43,10 @@ class OracleLocal:
     def sr_local_product(self, v):
         return self.oa.T @ (self.oa @ v)
 
+    def sr_local_product_device(self, v, z, stream):
+        import torch
+        z.copy_(torch.from_numpy(self.oa.T @ (self.oa @ v.numpy())))
+
     def sr_apply(self, mapping, x):
         self.applied = (np.asarray(mapping), np.asarray(x))
 
@@ -55,7 +59,7 @@ def inputs(tmp):
     return nl, init
 
 
-def _rank(rank, world, port, nl, init, out):
+def _rank(rank, world, port, nl, init, out, device_form=False):
     import torch
     import torch.distributed as dist
     import datetime
@@ -70,7 +74,10 @@ def _rank(rank, world, port, nl, init, out):
             dist.all_reduce(t)
             return t.numpy()
 
-        info = sharded.sr_step(local, reduce)
+        if device_form:
+            info = sharded.sr_step_device(local, reduce, dist.all_reduce, "cpu")
+        else:
+            info = sharded.sr_step(local, reduce)
         np.savez(os.path.join(out, f"rank{rank}.npz"), mapping=local.applied[0], x=local.applied[1],
                  info=np.array([info["nsmat"], info["info"]]))
     finally:
@@ -120,3 +127,27 @@ def test_cg_recurrence_statuses_match_oracle_on_fixed_operands():
         sto, xo, _ = ol.cg_fixed(mean, diag, o, g, 1.0 / ns, 1e-5, 0.0, limit, False)
         assert st == sto
         assert np.allclose(x, xo, rtol=1e-9, atol=1e-12)
+
+
+def _rank_device_form(rank, world, port, nl, init, out):
+    _rank(rank, world, port, nl, init, out, device_form=True)
+
+
+def test_two_gloo_ranks_with_tensor_vectors_match_the_array_form():
+    """sr_step_device (CG vectors as torch tensors, z reduced in place by all_reduce on the
+    tensor): both ranks apply identical updates, equal within the CG tolerance to the
+    array form on one process holding all chains, with the same active set."""
+    import torch.multiprocessing as mp
+    tmp = tempfile.mkdtemp()
+    nl, init = inputs(tmp)
+    port = 29600 + os.getpid() % 1000
+    mp.spawn(_rank_device_form, args=(2, port, nl, init, tmp), nprocs=2, join=True)
+    r0 = np.load(os.path.join(tmp, "rank0.npz"))
+    r1 = np.load(os.path.join(tmp, "rank1.npz"))
+    assert np.array_equal(r0["mapping"], r1["mapping"])
+    assert np.array_equal(r0["x"], r1["x"])
+    one = OracleLocal(nl, init, 4, 100)
+    info = sharded.sr_step(one, lambda a: a)
+    assert np.array_equal(one.applied[0], r0["mapping"]) and info["info"] >= 0 and int(r0["info"][1]) >= 0
+    scale = np.abs(one.applied[1]).max()
+    assert np.allclose(r0["x"], one.applied[1], rtol=1e-6, atol=1e-6 * scale)

@@ -46,6 +46,8 @@ struct GramSmem {
   uint64_t done;
   uint32_t tmem_base;
   int bad;
+  int issued;    // K slabs whose TMA loads were issued
+  int consumed;  // K slabs whose loads the MMA thread saw land
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -152,6 +154,8 @@ __global__ void __launch_bounds__(128, 1)
     }
     mbar_init(&sh.done, 1);
     sh.bad = 0;
+    sh.issued = 0;
+    sh.consumed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {  // 128 accumulator columns (FP32: one per output column)
@@ -178,6 +182,7 @@ __global__ void __launch_bounds__(128, 1)
       mbar_expect_tx(&sh.full[s], bm == bn ? kGramSlabBytes : 2 * kGramSlabBytes);
       tma_load_2d(sh.a[s], &map, kb * kstep, m0, &sh.full[s]);
       if (bm != bn) tma_load_2d(sh.b[s], &map, kb * kstep, n0, &sh.full[s]);
+      sh.issued = kb + 1;
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issue: four K steps of 32 bytes per slab (16 BF16 or 8 TF32 each)
@@ -189,6 +194,7 @@ __global__ void __launch_bounds__(128, 1)
         sh.bad = 1;
         break;
       }
+      sh.consumed = kb + 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a_addr = smem_u32(sh.a[s]);
       const uint32_t b_addr = bm == bn ? a_addr : smem_u32(sh.b[s]);
@@ -225,6 +231,11 @@ __global__ void __launch_bounds__(128, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if (sh.bad && threadIdx.x == 0) {
+    // after an expired wait: let the loads still in flight (issued, not seen to land by the
+    // MMA thread; at most one per stage) complete before the CTA's shared memory is released
+    for (int kb = sh.consumed; kb < sh.issued; ++kb) mbar_wait(&sh.full[kb % kGramStages], (kb / kGramStages) & 1);
+  }
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
 }

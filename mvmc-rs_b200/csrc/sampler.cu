@@ -139,10 +139,13 @@ __device__ __forceinline__ double log_proj_ratio_hop_warp(const DevModel& m, con
   if (m.n_jast > 0) {
     const double* vd = m.jast_pair + static_cast<size_t>(dest) * ns;
     const double* vs = m.jast_pair + static_cast<size_t>(source) * ns;
+    // loads outside the branch and unrolled, so that a lane's table loads are all in flight
+    // at once (the rows live in L2 for large lattices); the sum is the same as term by term
+#pragma unroll 8
     for (int k = lane; k < ns; k += 32) {
-      if (k == source || k == dest) continue;
-      const int x = num[k] + num[k + ns] - 1;
-      if (x != 0) z += (__ldg(vd + k) - __ldg(vs + k)) * static_cast<double>(x);
+      const int x = (k == source || k == dest) ? 0 : num[k] + num[k + ns] - 1;
+      const double d = __ldg(vd + k) - __ldg(vs + k);
+      if (x != 0) z += d * static_cast<double>(x);
     }
     z = warp_sum(z);
   }
@@ -237,17 +240,23 @@ __device__ __forceinline__ double log_ip_of(const DevModel& m, const double* pf,
 }
 
 // ---- Pfaffian ratio of a hop: pf_new[q] = -pf[q]·Σ_j InvM[q][msa][j]·S_q[rsa][rs_j] --------
+// The gathered Slater row stays in vec slot 0 for the update of an accepted hop.
 template <typename T>
 __device__ void ratio_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa) {
   const int n = m.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int rsa = rs_of(m, s.idx, msa);
-  // warps 1.. take the planes (warp 0 updates the projection counters meanwhile)
+  // warps 1.. take the planes (warp 0 forms Δln P meanwhile)
   const int pw = nwarp > 1 ? nwarp - 1 : 1, wi = nwarp > 1 ? warp - 1 : warp;
   if (wi < 0) return;
   for (int q = wi; q < m.nqp; q += pw) {
     const T* row = s.planes + (static_cast<size_t>(q) * n + msa) * n;
+    T* slt = s.vec + static_cast<size_t>(q) * 4 * n;
     T r = T(0);
-    for (int j = lane; j < n; j += 32) r += row[j] * slater_at<T>(m, q, rsa, rs_of(m, s.idx, j));
+    for (int j = lane; j < n; j += 32) {
+      const T sj = slater_at<T>(m, q, rsa, rs_of(m, s.idx, j));
+      slt[j] = sj;
+      r += row[j] * sj;
+    }
     r = warp_sum(r);
     if (lane == 0) s.pfn[q] = -static_cast<double>(r) * s.pf[q];
   }
@@ -394,17 +403,21 @@ __device__ __forceinline__ void col_dot2(const T* __restrict__ P, const T* __res
 // ---- rank-2 update of an accepted hop (update_one_real, updates.rs:1154-1215) --------------
 //   vec1 = −InvMᵀ·slt,  pf ← −pf·vec1[msa],  vec2 = InvM[msa]·(−1/vec1[msa]),
 //   InvM += vec1⊗vec2 − vec2⊗vec1, then column msa −= vec2 and row msa += vec2.
+// gathered: slt is already in vec slot 0 (ratio_hop_dev of the same proposal, followed by a
+// barrier).
 template <typename T, int JPL>
-__device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa) {
+__device__ void update_hop_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, bool gathered) {
   const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   const int rsa = rs_of(m, s.idx, msa);
   T* vec = s.vec;  // [q][0]=slt, [1]=vec1, [2]=vec2
-  for (int k = tid; k < nq * n; k += nt) {
-    const int q = k / n, i = k - q * n;
-    vec[(q * 4 + 0) * n + i] = slater_at<T>(m, q, rsa, rs_of(m, s.idx, i));
+  if (!gathered) {
+    for (int k = tid; k < nq * n; k += nt) {
+      const int q = k / n, i = k - q * n;
+      vec[(q * 4 + 0) * n + i] = slater_at<T>(m, q, rsa, rs_of(m, s.idx, i));
+    }
+    __syncthreads();
   }
-  __syncthreads();
   planes_col_dot(m, s, 0, 1);  // vec1
   __syncthreads();
   for (int k = tid; k < nq * n; k += nt) {
@@ -524,18 +537,24 @@ __device__ void ratio_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, in
 }
 
 // ---- rank-4 update of an accepted exchange (update_two_real, updates.rs:1429-1505) --------
+// gathered: va and vb of ratio_exchange_dev (same proposal) are still in vec slots 0 and 1;
+// only entry msb of vs differs from va.
 template <typename T, int JPL>
 __device__ void update_exchange_dev(const DevModel& m, const WalkerSmem<T>& s, int msa, int msb,
-                                    int rsa_old, int rsb_old) {
+                                    int rsa_old, int rsb_old, bool gathered) {
   const int n = m.n, nq = m.nqp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   const int rsa = rs_of(m, s.idx, msa), rsb = rs_of(m, s.idx, msb);
   T* vec = s.vec;  // [0]=vs, [1]=vt, [2]=vp, [3]=vq
-  for (int k = tid; k < nq * n; k += nt) {
-    const int q = k / n, i = k - q * n;
-    const int ri = rs_of(m, s.idx, i);
-    vec[(q * 4 + 0) * n + i] = (i == msb) ? slater_at<T>(m, q, rsa_old, rsb_old) : slater_at<T>(m, q, rsa, ri);
-    vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
+  if (gathered) {
+    for (int q = tid; q < nq; q += nt) vec[(q * 4 + 0) * n + msb] = slater_at<T>(m, q, rsa_old, rsb_old);
+  } else {
+    for (int k = tid; k < nq * n; k += nt) {
+      const int q = k / n, i = k - q * n;
+      const int ri = rs_of(m, s.idx, i);
+      vec[(q * 4 + 0) * n + i] = (i == msb) ? slater_at<T>(m, q, rsa_old, rsb_old) : slater_at<T>(m, q, rsa, ri);
+      vec[(q * 4 + 1) * n + i] = slater_at<T>(m, q, rsb, ri);
+    }
   }
   __syncthreads();
   // vp = InvM·vs, vq = InvM·vt in column form (skew symmetry)
@@ -955,9 +974,9 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
       lap(kPhMetropolis);
       if (cc[cAccept]) {
         if (type == 0) {
-          update_hop_dev<T, JPL>(m, s, msa);
+          update_hop_dev<T, JPL>(m, s, msa, true);
         } else {
-          update_exchange_dev<T, JPL>(m, s, msa, cc[cMsb], ri + sp * ns, rj + cc[cT] * ns);
+          update_exchange_dev<T, JPL>(m, s, msa, cc[cMsb], ri + sp * ns, rj + cc[cT] * ns, true);
         }
       }
       lap(kPhUpdate);
@@ -1203,11 +1222,11 @@ __global__ void __launch_bounds__(kStageThreads)
   } else if (op == kStageProposeHop) {
     ratio_hop_dev<double>(m, s, msa);
   } else if (op == kStageAcceptHop) {
-    update_hop_dev<double, JPL>(m, s, msa);
+    update_hop_dev<double, JPL>(m, s, msa, false);
   } else if (op == kStageProposeExchange) {
     ratio_exchange_dev<double, JPL>(m, s, msa, msb);
   } else if (op == kStageAcceptExchange) {
-    update_exchange_dev<double, JPL>(m, s, msa, msb, rsa_old, rsb_old);
+    update_exchange_dev<double, JPL>(m, s, msa, msb, rsa_old, rsb_old, false);
   }
   __syncthreads();
   for (int k = tid; k < m.nqp; k += blockDim.x) {

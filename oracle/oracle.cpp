@@ -114,16 +114,17 @@ struct Sfmt {
 // ===================================================================================
 #define A_(i, j) a[(i) + static_cast<size_t>(j) * n]
 
-int ltl_upper(double* a, int n, int* piv) {
+template <typename R>
+int ltl_upper(R* a, int n, int* piv) {
   int info = 0;
   for (int i = 0; i < n; ++i) piv[i] = i + 1;
   if (n < 2) return 0;
   for (int k0 = n - 1; k0 >= 1; --k0) {
     const int kk0 = k0 - 1;
     int kp = 0;
-    double colmax = 0.0;
+    R colmax = 0.0;
     for (int j = 0; j <= kk0; ++j) {
-      const double v = std::fabs(A_(j, k0));
+      const R v = std::fabs(A_(j, k0));
       if (j == 0 || v > colmax) {
         colmax = v;
         kp = j;
@@ -143,10 +144,10 @@ int ltl_upper(double* a, int n, int* piv) {
     }
     piv[kk0] = kp + 1;
     if (kk0 >= 1) {
-      const double alpha = 1.0 / A_(kk0, k0);
+      const R alpha = 1.0 / A_(kk0, k0);
       for (int j = 0; j < kk0; ++j) {
-        const double t1 = alpha * A_(j, kk0);
-        const double t2 = alpha * A_(j, k0);
+        const R t1 = alpha * A_(j, kk0);
+        const R t2 = alpha * A_(j, k0);
         for (int i = 0; i < j; ++i) A_(i, j) = (A_(i, j) + A_(i, k0) * t1) - A_(i, kk0) * t2;
         A_(j, j) = 0.0;
       }
@@ -156,8 +157,9 @@ int ltl_upper(double* a, int n, int* piv) {
   return info;
 }
 
-double ltl_pfaffian(const double* a, int n, const int* piv) {
-  double pf = 1.0;
+template <typename R>
+R ltl_pfaffian(const R* a, int n, const int* piv) {
+  R pf = 1.0;
   for (int i = 0; i + 1 < n; i += 2) pf *= A_(i, i + 1);
   bool neg = false;
   for (int k = 0; k < n; ++k)
@@ -165,17 +167,18 @@ double ltl_pfaffian(const double* a, int n, const int* piv) {
   return (neg ? -1.0 : 1.0) * pf;
 }
 
-void ltl_inverse(double* a, int n, const int* piv, std::vector<double>& mw, std::vector<double>& vt) {
+template <typename R>
+void ltl_inverse(R* a, int n, const int* piv, std::vector<R>& mw, std::vector<R>& vt) {
   mw.assign(static_cast<size_t>(n) * n, 0.0);
   vt.assign(n > 1 ? n - 1 : 1, 0.0);
-  double* m = mw.data();
+  R* m = mw.data();
 #define M_(i, j) m[(i) + static_cast<size_t>(j) * n]
   for (int i = 0; i < n; ++i) M_(i, i) = 1.0;
   // trtri of the unit upper block B(i, j) = A(i, j + 1), size n - 1.
   const int nb = n - 1;
   for (int j = 1; j < nb; ++j)
     for (int i = 0; i < j; ++i) {
-      double acc = A_(i, j + 1);
+      R acc = A_(i, j + 1);
       for (int k = i + 1; k < j; ++k) acc += A_(i, k + 1) * A_(k, j + 1);
       A_(i, j + 1) = -acc;
     }
@@ -184,8 +187,8 @@ void ltl_inverse(double* a, int n, const int* piv, std::vector<double>& mw, std:
   for (int i = 0; i < n - 1; ++i) vt[i] = -A_(i, i + 1);
   // skew-tridiagonal solve, direct divisions, output into A.
   for (int j = 0; j < n; ++j) {
-    const double* b = m + static_cast<size_t>(j) * n;
-    double* c = a + static_cast<size_t>(j) * n;
+    const R* b = m + static_cast<size_t>(j) * n;
+    R* c = a + static_cast<size_t>(j) * n;
     c[1] = b[0] / -vt[0];
     for (int i = 2; i < n; i += 2) c[i + 1] = (b[i] - c[i - 1] * vt[i - 1]) / -vt[i];
     c[n - 2] = b[n - 1] / vt[n - 2];
@@ -194,7 +197,7 @@ void ltl_inverse(double* a, int n, const int* piv, std::vector<double>& mw, std:
   auto trmm = [&]() {  // A <- M^T A, M unit upper
     for (int i = n - 1; i >= 0; --i)
       for (int j = 0; j < n; ++j) {
-        double acc = A_(i, j);
+        R acc = A_(i, j);
         for (int k = 0; k < i; ++k) acc += M_(k, i) * A_(k, j);
         A_(i, j) = acc;
       }
@@ -227,12 +230,13 @@ void ltl_inverse(double* a, int n, const int* piv, std::vector<double>& mw, std:
 #undef A_
 
 // In place: column-major X -> X^-1; returns 0 ok, >0 zero-pivot row, -1 non-finite Pf.
-int pfinv(double* a, int n, double* pf) {
+template <typename R>
+int pfinv(R* a, int n, R* pf) {
   std::vector<int> piv(n);
-  std::vector<double> mw, vt;
+  std::vector<R> mw, vt;
   const int info = ltl_upper(a, n, piv.data());
   if (info) return info;
-  const double p = ltl_pfaffian(a, n, piv.data());
+  const R p = ltl_pfaffian(a, n, piv.data());
   if (!std::isfinite(p)) return -1;
   *pf = p;
   ltl_inverse(a, n, piv.data(), mw, vt);
@@ -287,30 +291,32 @@ struct Ctx {
 };
 
 // Returns 0 ok; otherwise the plane's failure (pf/inv of later planes untouched).
-int calc_m_all(const Ctx& c, const int64_t* ele_idx, double* inv, double* pf) {
+template <typename R>
+int calc_m_all(const Ctx& c, const int64_t* ele_idx, R* inv, R* pf) {
   const int n = c.n;
-  std::vector<double> x(static_cast<size_t>(n) * n);
+  std::vector<R> x(static_cast<size_t>(n) * n);
   for (int q = 0; q < c.nqp; ++q) {
-    double maxabs = 0.0;
+    R maxabs = 0.0;
     for (int msi = 0; msi < n; ++msi)
       for (int msj = 0; msj < n; ++msj) {
-        const double v = -c.S(q, c.rs(ele_idx, msi), c.rs(ele_idx, msj));
+        const R v = -c.S(q, c.rs(ele_idx, msi), c.rs(ele_idx, msj));
         x[msj + static_cast<size_t>(msi) * n] = v;
         maxabs = std::max(maxabs, v * v);
       }
     if (maxabs < 1e-300) return 1000000 + q;
-    double p = 0.0;
+    R p = 0.0;
     const int st = pfinv(x.data(), n, &p);
     if (st) return st;
     pf[q] = p;
-    double* dst = inv + static_cast<size_t>(q) * n * n;
+    R* dst = inv + static_cast<size_t>(q) * n * n;
     for (size_t k = 0; k < x.size(); ++k) dst[k] = -x[k];
   }
   return 0;
 }
 
-double ip_of(const Ctx& c, const double* pf) {  // calculate_ip_real (observables.rs:128)
-  double ip = 0.0;
+template <typename R>
+R ip_of(const Ctx& c, const R* pf) {  // calculate_ip_real (observables.rs:128)
+  R ip = 0.0;
   for (int q = 0; q < c.nqp; ++q) ip += c.m.qp_weight[q] * pf[q];
   return ip;
 }
@@ -394,31 +400,33 @@ void revert_ele_config(const Ctx& c, int mi, int ri, int rj, int s, int64_t* idx
 // Ratios and rank-2 / rank-4 updates (sampling/updates.rs:73-160,395-444,588-640,
 // 779-835,984-1086,1154-1215,1429-1505,1539-1622)
 // ===================================================================================
-void ratio_hop(const Ctx& c, int msa, const int64_t* idx, const double* inv, const double* pf,
-               double* pf_new) {
+template <typename R>
+void ratio_hop(const Ctx& c, int msa, const int64_t* idx, const R* inv, const R* pf,
+               R* pf_new) {
   const int n = c.n;
   const int rsa = c.rs(idx, msa);
   for (int q = 0; q < c.nqp; ++q) {
-    const double* row = inv + static_cast<size_t>(q) * n * n + static_cast<size_t>(msa) * n;
-    double r = 0.0;
+    const R* row = inv + static_cast<size_t>(q) * n * n + static_cast<size_t>(msa) * n;
+    R r = 0.0;
     for (int j = 0; j < n; ++j) r += row[j] * c.S(q, rsa, c.rs(idx, j));
     pf_new[q] = -r * pf[q];
   }
 }
 
-void update_hop(const Ctx& c, int msa, const int64_t* idx, double* inv, double* pf) {
+template <typename R>
+void update_hop(const Ctx& c, int msa, const int64_t* idx, R* inv, R* pf) {
   const int n = c.n;
   const int rsa = c.rs(idx, msa);
-  std::vector<double> slt(n), v1(n), v2(n);
+  std::vector<R> slt(n), v1(n), v2(n);
   for (int q = 0; q < c.nqp; ++q) {
-    double* m = inv + static_cast<size_t>(q) * n * n;
+    R* m = inv + static_cast<size_t>(q) * n * n;
     for (int j = 0; j < n; ++j) slt[j] = c.S(q, rsa, c.rs(idx, j));
     std::fill(v1.begin(), v1.end(), 0.0);
     for (int i = 0; i < n; ++i)
       for (int j = 0; j < n; ++j) v1[j] += -m[i * n + j] * slt[i];
-    const double tmp = v1[msa];
+    const R tmp = v1[msa];
     pf[q] *= -tmp;
-    const double inv_a = -1.0 / tmp;
+    const R inv_a = -1.0 / tmp;
     for (int j = 0; j < n; ++j) v2[j] = m[msa * n + j] * inv_a;
     for (int i = 0; i < n; ++i) {
       for (int j = 0; j < n; ++j) m[i * n + j] += v1[i] * v2[j] - v1[j] * v2[i];
@@ -428,46 +436,48 @@ void update_hop(const Ctx& c, int msa, const int64_t* idx, double* inv, double* 
   }
 }
 
-void ratio_exchange(const Ctx& c, int msa, int msb, const int64_t* idx, const double* inv,
-                    const double* pf, double* pf_new) {
+template <typename R>
+void ratio_exchange(const Ctx& c, int msa, int msb, const int64_t* idx, const R* inv,
+                    const R* pf, R* pf_new) {
   const int n = c.n;
   const int rsa = c.rs(idx, msa), rsb = c.rs(idx, msb);
-  std::vector<double> va(n), vb(n);
+  std::vector<R> va(n), vb(n);
   for (int q = 0; q < c.nqp; ++q) {
-    const double* m = inv + static_cast<size_t>(q) * n * n;
+    const R* m = inv + static_cast<size_t>(q) * n * n;
     for (int i = 0; i < n; ++i) {
       va[i] = c.S(q, rsa, c.rs(idx, i));
       vb[i] = c.S(q, rsb, c.rs(idx, i));
     }
-    const double vba = vb[msa];
-    double pa = 0, pb = 0, qa = 0, qb = 0;
+    const R vba = vb[msa];
+    R pa = 0, pb = 0, qa = 0, qb = 0;
     for (int i = 0; i < n; ++i) {
       pa += m[msa * n + i] * va[i];
       pb += m[msb * n + i] * va[i];
       qa += m[msa * n + i] * vb[i];
       qb += m[msb * n + i] * vb[i];
     }
-    const double iab = m[msa * n + msb];
-    double bma = 0.0;
+    const R iab = m[msa * n + msb];
+    R bma = 0.0;
     for (int i = 0; i < n; ++i) {
-      double t = 0.0;
+      R t = 0.0;
       for (int j = 0; j < n; ++j) t += m[i * n + j] * va[j];
       bma += vb[i] * t;
     }
-    const double ratio = iab * vba + iab * bma + pa * qb - pb * qa;
+    const R ratio = iab * vba + iab * bma + pa * qb - pb * qa;
     pf_new[q] = ratio * pf[q];
   }
 }
 
+template <typename R>
 void update_exchange(const Ctx& c, int msa, int msb, int ra_old, int rb_old, int sa, int sb,
-                     const int64_t* idx, double* inv, double* pf) {
+                     const int64_t* idx, R* inv, R* pf) {
   const int n = c.n;
   const int rsa = c.rs(idx, msa), rsb = c.rs(idx, msb);
   const int rsa_old = ra_old + sa * c.ns, rsb_old = rb_old + sb * c.ns;
-  std::vector<double> vs(n), vt(n), vp(n), vq(n);
+  std::vector<R> vs(n), vt(n), vp(n), vq(n);
   for (int qp = 0; qp < c.nqp; ++qp) {
-    double* m = inv + static_cast<size_t>(qp) * n * n;
-    const double m_old_ab = c.S(qp, rsa_old, rsb_old);
+    R* m = inv + static_cast<size_t>(qp) * n * n;
+    const R m_old_ab = c.S(qp, rsa_old, rsb_old);
     for (int i = 0; i < n; ++i) {
       vs[i] = c.S(qp, rsa, c.rs(idx, i));
       vt[i] = c.S(qp, rsb, c.rs(idx, i));
@@ -480,23 +490,23 @@ void update_exchange(const Ctx& c, int msa, int msb, int ra_old, int rb_old, int
         vp[i] += m[i * n + j] * vs[j];
         vq[i] += m[i * n + j] * vt[j];
       }
-    double bma = 0.0;
+    R bma = 0.0;
     for (int i = 0; i < n; ++i) bma += vt[i] * vp[i];
-    const double iab = m[msa * n + msb];
-    const double ratio = iab * vt[msa] + iab * bma + vp[msa] * vq[msb] - vp[msb] * vq[msa];
+    const R iab = m[msa * n + msb];
+    const R ratio = iab * vt[msa] + iab * bma + vp[msa] * vq[msb] - vp[msb] * vq[msa];
     pf[qp] *= ratio;
-    const double a = -vp[msa], b = vp[msb], cc = vq[msa], d = -vq[msb];
-    const double e = -bma - vt[msa], f = iab;
-    const double det = a * d - b * cc - e * f;
-    const double idet = 1.0 / det;
+    const R a = -vp[msa], b = vp[msb], cc = vq[msa], d = -vq[msb];
+    const R e = -bma - vt[msa], f = iab;
+    const R det = a * d - b * cc - e * f;
+    const R idet = 1.0 / det;
     for (int i = 0; i < n; ++i) {
       vs[i] = idet * m[msa * n + i];
       vt[i] = idet * m[msb * n + i];
     }
     for (int i = 0; i < n; ++i) {
-      const double pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
+      const R pi = vp[i], qi = vq[i], si = vs[i], ti = vt[i];
       for (int j = 0; j < n; ++j) {
-        const double pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
+        const R pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
         m[i * n + j] += a * (qi * tj - qj * ti) + b * (qi * sj - qj * si) + cc * (pi * tj - pj * ti) +
                         d * (pi * sj - pj * si) + e * det * (si * tj - sj * ti) +
                         f * idet * (pi * qj - qi * pj);
@@ -505,7 +515,7 @@ void update_exchange(const Ctx& c, int msa, int msb, int ra_old, int rb_old, int
       m[i * n + msb] += -a * ti - b * si + f * idet * pi;
     }
     for (int j = 0; j < n; ++j) {
-      const double pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
+      const R pj = vp[j], qj = vq[j], sj = vs[j], tj = vt[j];
       m[msa * n + j] += cc * tj + d * sj + f * idet * qj;
       m[msb * n + j] += a * tj + b * sj - f * idet * pj;
     }
@@ -556,6 +566,72 @@ double g_refresh_drift = 0.0;
 // lies outside [g, 1/g] (0 = off, the reference's schedule); counts guard refreshes.
 double g_guard = 0.0;
 long long g_guard_count = 0, g_sched_count = 0;
+
+// Teacher-forced long-double shadow of one FP64 chain (oracle_trace_chain): the same
+// proposals, decisions and refresh points as the FP64 chain, with the Pfaffians and inverses
+// carried in long double by the same algorithms (64-bit significand: 2^11 times the
+// precision of double), and the chain's stage operations recorded for a device replay.
+// Record per op (8 doubles): PROPOSE: dproj, u, 2((dproj + ln|IP'|) - ln|IP|) in FP64 and in
+// long double, accepted, ln|IP| tracked in FP64 and in long double, min_q |pf'_q/pf_q|;
+// RECOMPUTE: ln|IP| tracked in FP64 before, recomputed in FP64, recomputed in long double,
+// tracked in long double before.
+struct Tracer {
+  using LD = long double;
+  std::vector<LD> inv, pf, pfn;
+  LD lip = 0, lip_new = 0;
+  std::vector<int32_t> ops;
+  std::vector<int64_t> cands;
+  std::vector<double> rec;
+  size_t max_ops = 0;
+  bool full() const { return ops.size() / 7 >= max_ops; }
+  void push(const Ctx& c, int code, int ma, int sa, int mb, int sb, int ra, int rb, const int64_t* idx,
+            const double* r) {
+    if (full()) return;
+    const int32_t o[7] = {code, ma, sa, mb, sb, ra, rb};
+    ops.insert(ops.end(), o, o + 7);
+    cands.insert(cands.end(), idx, idx + c.n);
+    rec.insert(rec.end(), r, r + 8);
+  }
+  LD log_ip_ld(const Ctx& c, const LD* p) const { return std::log(std::fabs(ip_of(c, p))); }
+  void begin(const Ctx& c, const int64_t* idx) {
+    inv.assign(static_cast<size_t>(c.nqp) * c.n * c.n, 0);
+    pf.assign(c.nqp, 0);
+    pfn.assign(c.nqp, 0);
+    if (calc_m_all(c, idx, inv.data(), pf.data()) != 0) throw std::runtime_error("trace: singular start");
+    lip = log_ip_ld(c, pf.data());
+  }
+  void propose(const Ctx& c, int type, int msa, int msb, const int64_t* idx, double dproj, double u,
+               double lw64, bool acc, double lip64, const double* pf_new64, const double* pf64) {
+    if (type == 0) ratio_hop(c, msa, idx, inv.data(), pf.data(), pfn.data());
+    else ratio_exchange(c, msa, msb, idx, inv.data(), pf.data(), pfn.data());
+    lip_new = log_ip_ld(c, pfn.data());
+    const LD lw = 2.0L * ((static_cast<LD>(dproj) + lip_new) - lip);
+    double rmin = 1e300;
+    for (int q = 0; q < c.nqp; ++q) rmin = std::min(rmin, std::fabs(pf_new64[q] / pf64[q]));
+    const double r[8] = {dproj, u, lw64, static_cast<double>(lw), acc ? 1.0 : 0.0, lip64,
+                         static_cast<double>(lip), rmin};
+    const int ne = c.ne;
+    if (type == 0) push(c, 0, msa % ne, msa / ne, 0, 0, 0, 0, idx, r);
+    else push(c, 2, msa % ne, msa / ne, msb % ne, msb / ne, 0, 0, idx, r);
+  }
+  void accept(const Ctx& c, int type, int msa, int msb, int ri, int rj, int sa, int sb, const int64_t* idx) {
+    if (type == 0) update_hop(c, msa, idx, inv.data(), pf.data());
+    else update_exchange(c, msa, msb, ri, rj, sa, sb, idx, inv.data(), pf.data());
+    lip = lip_new;
+    const double r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int ne = c.ne;
+    if (type == 0) push(c, 1, msa % ne, msa / ne, 0, 0, 0, 0, idx, r);
+    else push(c, 3, msa % ne, msa / ne, msb % ne, msb / ne, ri, rj, idx, r);
+  }
+  void recompute(const Ctx& c, const int64_t* idx, double tracked64, double fresh64) {
+    const LD before = lip;
+    if (calc_m_all(c, idx, inv.data(), pf.data()) != 0) throw std::runtime_error("trace: singular refresh");
+    lip = log_ip_ld(c, pf.data());
+    const double r[8] = {tracked64, fresh64, static_cast<double>(lip), static_cast<double>(before), 0, 0, 0, 0};
+    push(c, 4, 0, 0, 0, 0, 0, 0, idx, r);
+  }
+};
+Tracer* g_tracer = nullptr;
 
 bool guard_trips(const Ctx& c, const double* pf_new, const double* pf_old) {
   if (g_guard <= 0.0) return false;
@@ -609,9 +685,13 @@ void run_block(const Ctx& c, Walker& w, int n_in, double& log_ip_old, int& n_acc
       double wgt = std::exp(2.0 * ((dproj + 0.0 + lip_new) - log_ip_old));
       if (!std::isfinite(wgt)) wgt = -1.0;
       const double u = w.rng.real2();
+      if (g_tracer)
+        g_tracer->propose(c, 0, msa, 0, idx, dproj, u, 2.0 * ((dproj + 0.0 + lip_new) - log_ip_old), wgt > u,
+                          log_ip_old, pf_new.data(), w.pf.data());
       if (wgt > u) {
         const bool trip = guard_trips(c, pf_new.data(), w.pf.data());
         update_hop(c, msa, idx, w.inv.data(), w.pf.data());
+        if (g_tracer) g_tracer->accept(c, 0, msa, 0, ri, rj, s, s, idx);
         w.proj_cnt = cnt_new;
         log_ip_old = lip_new;
         ++n_acc_win;
@@ -658,9 +738,13 @@ void run_block(const Ctx& c, Walker& w, int n_in, double& log_ip_old, int& n_acc
       double wgt = std::exp(2.0 * ((dproj + 0.0 + lip_new) - log_ip_old));
       if (!std::isfinite(wgt)) wgt = -1.0;
       const double u = w.rng.real2();
+      if (g_tracer)
+        g_tracer->propose(c, 1, msa, msb, idx, dproj, u, 2.0 * ((dproj + 0.0 + lip_new) - log_ip_old), wgt > u,
+                          log_ip_old, pf_new.data(), w.pf.data());
       if (wgt > u) {
         const bool trip = guard_trips(c, pf_new.data(), w.pf.data());
         update_exchange(c, msa, msb, ri, rj, s, t, idx, w.inv.data(), w.pf.data());
+        if (g_tracer) g_tracer->accept(c, 1, msa, msb, ri, rj, s, t, idx);
         w.proj_cnt = cnt_new;
         log_ip_old = lip_new;
         ++n_acc_win;
@@ -682,6 +766,7 @@ void run_block(const Ctx& c, Walker& w, int n_in, double& log_ip_old, int& n_acc
         const double fresh = log_ip(c, w.pf.data());
         const double d = std::fabs(fresh - log_ip_old);
         if (std::isfinite(d) && d > g_refresh_drift) g_refresh_drift = d;
+        if (g_tracer) g_tracer->recompute(c, idx, log_ip_old, fresh);
         log_ip_old = fresh;
       }
       n_acc_win = 0;
@@ -1847,6 +1932,63 @@ int oracle_opt_step1_walkers(const char* namelist, const char* initial_def, int 
     energy[4] = tot.sztot2;
     std::copy(tot.ho.begin(), tot.ho.end(), ho);
     std::copy(tot.oo.begin(), tot.oo.end(), oo);
+    return 0;
+  } catch (const std::exception& e) {
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
+}
+
+int oracle_trace_chain(const char* namelist, const char* initial_def, long long seed, int walker, int blocks,
+                       int max_ops, int64_t* idx0, int32_t* ops, int64_t* cands, double* rec, int* nops,
+                       char* err, int err_len) {
+  orc::Tracer tr;
+  try {
+    mvmc::Model m = mvmc::read_expert(namelist);
+    if (m.nsrcg == 0) m.nsrcg = 1;
+    std::vector<orc::Walker> ws(static_cast<size_t>(std::max(0, walker)) + 1);
+    orc::seed_walkers(m, ws, seed >= 0 ? seed : m.rnd_seed);
+    if (initial_def && *initial_def) {
+      std::string why;
+      if (!mvmc::read_para_triples(m, initial_def, &why)) throw std::runtime_error("initial.def: " + why);
+    }
+    mvmc::sync_modified_parameter(m, true);
+    mvmc::init_qp_weight(m);
+    std::vector<double> slater;
+    mvmc::build_slater_table(m, slater);
+    orc::Ctx c(m, slater);
+    orc::Walker& w = ws.back();
+    orc::init_walker(c, w);
+    orc::initial_with_retry(c, w);
+    orc::calc_m_all(c, w.ele_idx.data(), w.inv.data(), w.pf.data());
+    double lip = orc::log_ip(c, w.pf.data());
+    if (!std::isfinite(lip)) throw std::runtime_error("trace: non-finite initial amplitude");
+    std::copy(w.ele_idx.begin(), w.ele_idx.end(), idx0);
+    tr.max_ops = static_cast<size_t>(std::max(0, max_ops));
+    tr.begin(c, w.ele_idx.data());
+    const int n_out = std::min(blocks, c.m.nvmc_warmup + c.m.nvmc_sample);
+    const int n_in = c.m.nvmc_interval * std::max(1, c.ns);
+    int n_acc_win = 0;
+    orc::g_tracer = &tr;
+    for (int out = 0; out < n_out && !tr.full(); ++out) orc::run_block(c, w, n_in, lip, n_acc_win);
+    orc::g_tracer = nullptr;
+    std::copy(tr.ops.begin(), tr.ops.end(), ops);
+    std::copy(tr.cands.begin(), tr.cands.end(), cands);
+    std::copy(tr.rec.begin(), tr.rec.end(), rec);
+    *nops = static_cast<int>(tr.ops.size() / 7);
+    return 0;
+  } catch (const std::exception& e) {
+    orc::g_tracer = nullptr;
+    orc::copy_err(e, err, err_len);
+    return 1;
+  }
+}
+
+int oracle_qp_weights(const char* namelist, double* out, char* err, int err_len) {
+  try {
+    mvmc::Model m = mvmc::read_expert(namelist);
+    mvmc::init_qp_weight(m);
+    std::copy(m.qp_weight.begin(), m.qp_weight.end(), out);
     return 0;
   } catch (const std::exception& e) {
     orc::copy_err(e, err, err_len);

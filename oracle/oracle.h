@@ -99,6 +99,22 @@ int oracle_stage_replay(const char* namelist, const double* params, int npara, c
                         const int* ops, const int64_t* idx_seq, double* out, double* inv_out, char* err,
                         int err_len);
 
+// One FP64 chain (walker `walker` of the first SR step: RndSeed + walker, parameters as in
+// oracle_opt_step1_walkers) run for min(blocks, warm-up + samples) blocks with a long-double
+// shadow of its Pfaffians and inverses, teacher-forced on the FP64 decisions. Returns the
+// start configuration idx0[n] and the chain's stage operations in the format of
+// oracle_stage_replay (ops[7k..], candidate configurations cands[k*n..]), at most max_ops,
+// with rec[8k..]: for a proposal {dproj, u, log-weight FP64, log-weight long double,
+// accepted, ln|IP| tracked FP64, ln|IP| tracked long double, min_q |pf'_q/pf_q|}; for a
+// recompute {ln|IP| tracked FP64 before, recomputed FP64, recomputed long double, tracked
+// long double before}; zeros for accepts.
+int oracle_trace_chain(const char* namelist, const char* initial_def, long long seed, int walker, int blocks,
+                       int max_ops, int64_t* idx0, int32_t* ops, int64_t* cands, double* rec, int* nops,
+                       char* err, int err_len);
+
+// The QP weights of the model (init_qp_weight): out[nqp].
+int oracle_qp_weights(const char* namelist, double* out, char* err, int err_len);
+
 // Largest |ln|IP|_recomputed − ln|IP|_tracked| at a sampler refresh since the last reset
 // (the FP64 rank-2 updates' drift on the C refresh schedule); reset != 0 clears it.
 double oracle_refresh_drift(int reset);

@@ -178,6 +178,33 @@ def opt_step1_walkers(namelist, walkers, seed=-1, initial_def=""):
     return d, out
 
 
+def trace_chain(namelist, walker, blocks, max_ops, seed=-1, initial_def=""):
+    """One FP64 oracle chain with its long-double shadow (oracle_trace_chain): returns
+    (idx0[n], ops[k][7], cands[k][n], rec[k][8])."""
+    d = model_dims(namelist)
+    n = 2 * d["ne"]
+    idx0 = np.zeros(n, np.int64)
+    ops = np.zeros((max_ops, 7), np.int32)
+    cands = np.zeros((max_ops, n), np.int64)
+    rec = np.zeros((max_ops, 8))
+    k = ctypes.c_int(0)
+    err = err_buf()
+    rc = lib().oracle_trace_chain(namelist.encode(), initial_def.encode(), ctypes.c_longlong(seed), walker, blocks,
+                                  max_ops, ptr(idx0), ptr(ops), ptr(cands), ptr(rec), ctypes.byref(k), err, 1024)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    k = k.value
+    return idx0, ops[:k], cands[:k], rec[:k]
+
+
+def qp_weights(namelist):
+    out = np.zeros(model_dims(namelist)["nqp"])
+    err = err_buf()
+    if lib().oracle_qp_weights(namelist.encode(), ptr(out), err, 1024) != 0:
+        raise RuntimeError(err.value.decode())
+    return out
+
+
 def stage_replay(namelist, params, idx0, ops, idx_seq, nqp, n):
     """Teacher-forced replay of the stage operations; returns (out[nops][nqp], inv[nqp][n][n])."""
     params = np.ascontiguousarray(params, dtype=np.float64)

@@ -328,6 +328,225 @@ __global__ void __launch_bounds__(G * G, (G == 8 ? (sizeof(T) == 8 ? 4 : 6) : (G
   }
 }
 
+// Uniform batches of side N ∈ {32, 64}: the register sweep with one barrier per pivot step.
+// Thread (tr, tc) of a G×G block owns the R×R elements (tr + G·a, tc + G·b), R = N/G. At
+// the barrier of step k shared memory holds the current rows p_k and q_k and the current
+// row of the next pivot index p_{k+1}; every thread then (1) applies the rank-2 update of
+// step k to its elements, (2) recomputes row p_{k+1} after the update in registers (every
+// warp the whole row, N/32 columns per lane, from the three published rows) and finds its
+// pivot q_{k+1} by the first-maximum rule with a warp reduction — all warps get the same
+// bits, so no barrier is needed to agree on it — and (3) the owners of rows q_{k+1} and
+// p_{k+2} publish them (warp 0 publishes row p_{k+1}) into the other buffer set. Rows and
+// columns p, q are overwritten after each update (as in k_pfinv_reg), so the owners' copies
+// of row p_{k+1} are never read: only the recomputed row is used.
+template <typename T, int N, int G, int MB>
+__global__ void __launch_bounds__(G * G, MB)
+    k_pfinv_uni(const double* __restrict__ x, int planes, double* __restrict__ pf, double* __restrict__ inv,
+                int* __restrict__ status) {
+  static_assert(N == 32 || N == 64, "one 64-bit swept mask, whole warps per row pass");
+  constexpr int R = N / G, NT = G * G, C = N / 32, LDA = N + 1;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* stage = reinterpret_cast<T*>(smem);  // [N][N + 1]
+  T* bufs = stage + N * LDA;              // [2 parities][3 rows: p, q, next p][N]
+  const int tid = threadIdx.x, tr = tid / G, tc = tid % G, lane = tid & 31;
+  const unsigned long long all = N == 64 ? ~0ull : ((1ull << N) - 1ull);
+  for (int plane = blockIdx.x; plane < planes; plane += gridDim.x) {
+    const double* xp = x + static_cast<size_t>(plane) * N * N;
+    double* ip = inv + static_cast<size_t>(plane) * N * N;
+    for (int k = tid; k < N * N; k += NT) stage[(k / N) * LDA + k % N] = static_cast<T>(-xp[k]);
+    __syncthreads();
+    T e[R][R];
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = 0; b < R; ++b) e[a][b] = stage[(tr + G * a) * LDA + tc + G * b];
+    // first maximum of |row[j]| over unswept j ≠ r (values v[c] at j = lane + 32c), the
+    // pivot value and the number of unswept indices strictly between r and the pivot
+    auto pivot = [&](const T* v, int r, unsigned long long sw, int& q, T& av, int& cnt) {
+      double best = -1.0;
+      int bi = N;
+      T bval = T(0);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int j = lane + 32 * c;
+        if (j != r && !((sw >> j) & 1ull)) {
+          const double a = fabs(static_cast<double>(v[c]));
+          if (a > best) {
+            best = a;
+            bi = j;
+            bval = v[c];
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        const T ov = __shfl_xor_sync(0xffffffffu, bval, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+          bval = ov;
+        }
+      }
+      q = best > 0.0 ? bi : N;
+      av = bval;
+      cnt = 0;
+      if (q < N && q > r + 1) {
+        const int len = q - r - 1;
+        const unsigned long long range = (len == 64 ? ~0ull : ((1ull << len) - 1ull)) << (r + 1);
+        cnt = __popcll(~sw & range);
+      }
+    };
+    auto lowest_unswept = [&](unsigned long long sw) {
+      const unsigned long long free = ~sw & all;
+      return free ? __ffsll(static_cast<long long>(free)) - 1 : N;
+    };
+    // step 0: rows straight from the staged matrix
+    unsigned long long sw = 0ull;
+    int p = 0, q, cnt, st = 0, parity = 0;
+    T av;
+    {
+      T v[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[c] = stage[lane + 32 * c];
+      pivot(v, 0, sw, q, av, cnt);
+    }
+    double pfv = 1.0;
+    const T* rP = stage;
+    const T* rQ = stage + (q < N ? q : 0) * LDA;
+    int pn = lowest_unswept(sw | 1ull | (q < N ? (1ull << q) : 0ull));
+    const T* rN = stage + (pn < N ? pn : 0) * LDA;
+    for (int k = 0; k < N / 2; ++k) {
+      if (q >= N) {
+        st = p + 1;
+        break;
+      }
+      const T ia = T(1) / av;
+      parity += cnt;
+      pfv *= static_cast<double>(av);
+      // (1) rank-2 update of step k, then columns and rows p, q
+      T rpj[R], rqj[R];
+#pragma unroll
+      for (int b = 0; b < R; ++b) {
+        rpj[b] = rP[tc + G * b];
+        rqj[b] = rQ[tc + G * b];
+      }
+#pragma unroll
+      for (int a = 0; a < R; ++a) {
+        const int i = tr + G * a;
+        const T rpi = rP[i] * ia, rqi = rQ[i] * ia;
+#pragma unroll
+        for (int b = 0; b < R; ++b) e[a][b] += rqi * rpj[b] - rpi * rqj[b];
+      }
+      if (tc == p % G || tc == q % G) {
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+          const int j = tc + G * b;
+          if (j != p && j != q) continue;
+#pragma unroll
+          for (int a = 0; a < R; ++a) {
+            const int i = tr + G * a;
+            e[a][b] = j == p ? -rQ[i] * ia : rP[i] * ia;
+          }
+        }
+      }
+      if (tr == p % G || tr == q % G) {
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+          const int i = tr + G * a;
+          if (i != p && i != q) continue;
+#pragma unroll
+          for (int b = 0; b < R; ++b) {
+            const int j = tc + G * b;
+            if (i == p) e[a][b] = (j == q) ? -ia : (j == p ? T(0) : rqj[b] * ia);
+            else e[a][b] = (j == p) ? ia : (j == q ? T(0) : -rpj[b] * ia);
+          }
+        }
+      }
+      sw |= (1ull << p) | (1ull << q);
+      if (k == N / 2 - 1) break;
+      // (2) row p' = pn after this update, in every warp, and its pivot
+      T v[C];
+      {
+        const T rpp = rP[pn] * ia, rqp = rQ[pn] * ia;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int j = lane + 32 * c;
+          T val = rN[j] + (rqp * rP[j] - rpp * rQ[j]);
+          if (j == p) val = -rQ[pn] * ia;
+          if (j == q) val = rP[pn] * ia;
+          v[c] = val;
+        }
+      }
+      int qn, cn;
+      T an;
+      pivot(v, pn, sw, qn, an, cn);
+      const int pnn = qn < N ? lowest_unswept(sw | (1ull << pn) | (1ull << qn)) : N;
+      // (3) publish rows p', q' and the next p'' into the other buffer set
+      T* oP = bufs + ((k + 1) & 1) * 3 * N;
+      T* oQ = oP + N;
+      T* oN = oQ + N;
+      if (tid < 32) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) oP[lane + 32 * c] = v[c];
+      }
+      if (qn < N && tr == qn % G) {
+        const int aq = qn / G;
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+          if (a != aq) continue;
+#pragma unroll
+          for (int b = 0; b < R; ++b) oQ[tc + G * b] = e[a][b];
+        }
+      }
+      if (pnn < N && tr == pnn % G) {
+        const int an2 = pnn / G;
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+          if (a != an2) continue;
+#pragma unroll
+          for (int b = 0; b < R; ++b) oN[tc + G * b] = e[a][b];
+        }
+      }
+      __syncthreads();
+      rP = oP;
+      rQ = oQ;
+      rN = oN;
+      p = pn;
+      q = qn;
+      av = an;
+      cnt = cn;
+      pn = pnn;
+    }
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = 0; b < R; ++b) ip[static_cast<size_t>(tr + G * a) * N + tc + G * b] = -static_cast<double>(e[a][b]);
+    if (tid == 0) {
+      double val = (parity & 1) ? -pfv : pfv;
+      if (st == 0 && !isfinite(val)) st = -1;
+      if (st != 0) val = 0.0;
+      pf[plane] = val;
+      status[plane] = st;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, int N, int G, int MB>
+int launch_pfinv_uni(const double* x, int planes, double* pf, double* inv, int* status, cudaStream_t stream) {
+  const size_t smem = sizeof(T) * (static_cast<size_t>(N) * (N + 1) + 6 * static_cast<size_t>(N));
+  auto kernel = k_pfinv_uni<T, N, G, MB>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 0;
+  MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G * G, smem));
+  const int grid = std::max(1, std::min(planes, std::max(1, per_sm) * device_sm_count()));
+  kernel<<<grid, G * G, smem, stream>>>(x, planes, pf, inv, status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
 template <typename T, int G, int R>
 int launch_pfinv_reg(const double* x, const int* sizes, const long long* offsets, int n_uniform, int planes,
                      int n_max, double* pf, double* inv, int* status, cudaStream_t stream) {
@@ -465,6 +684,18 @@ int pfinv_device(const double* x, const int* sizes, const long long* offsets, in
   if (planes <= 0) return kOk;
   if (n_max <= 0 || (n_max & 1) || !x || !pf || !inv || !status) return kErrArgument;
   const int limit = device_smem_limit();
+  if (!sizes && n_uniform == n_max && (n_max == 32 || n_max == 64) && (precision == 32 || precision == 64) &&
+      !std::getenv("MVMC_B200_PFINV_TILE")) {
+    // uniform batches of 32 or 64: one barrier per pivot step (MVMC_B200_PFINV_TILE keeps
+    // the two-barrier tiles)
+    // (measured at B = 8192, n = 64: 1.31 ms FP64 / 1.03 ms FP32 against 1.49 / 1.16 ms for the
+    // two-barrier 16×4 tile; same bits; capping registers for two blocks per SM is slower)
+    if (precision == 32)
+      return n_max == 32 ? launch_pfinv_uni<float, 32, 16, 4>(x, planes, pf, inv, status, stream)
+                         : launch_pfinv_uni<float, 64, 16, 4>(x, planes, pf, inv, status, stream);
+    return n_max == 32 ? launch_pfinv_uni<double, 32, 16, 3>(x, planes, pf, inv, status, stream)
+                       : launch_pfinv_uni<double, 64, 16, 3>(x, planes, pf, inv, status, stream);
+  }
   if (n_max <= 128 && (precision == 32 || precision == 64)) {
     if (precision == 32)
       return dispatch_pfinv_reg<float>(x, sizes, offsets, n_uniform, planes, n_max, pf, inv, status, stream);

@@ -118,3 +118,52 @@ def test_autotuner_candidates_give_identical_bits(n, tiles, precision, monkeypat
         for a, b in zip(base, got):
             assert np.array_equal(a, b), t
     monkeypatch.setenv("MVMC_B200_PFINV_TILE", "")
+
+
+def device_uniform(xc, n, planes, precision):
+    """mvmc_b200_pfinv_batch_device on a uniform batch (sizes NULL) in device buffers."""
+    import ctypes
+    import torch
+    x = torch.from_numpy(np.ascontiguousarray(xc)).cuda()
+    inv = torch.empty_like(x)
+    pf = torch.zeros(planes, dtype=torch.float64, device="cuda")
+    st = torch.zeros(planes, dtype=torch.int32, device="cuda")
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = mvmc().lib().mvmc_b200_pfinv_batch_device(P(x), None, None, n, planes, n, P(pf), P(inv), P(st), precision,
+                                                   None)
+    assert rc >= 0
+    torch.cuda.synchronize()
+    return pf.cpu().numpy(), inv.cpu().numpy(), st.cpu().numpy()
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_uniform_batch_kernel_matches_oracle_and_flags_singular_planes(n):
+    """Uniform batches of side 32 and 64 run the one-barrier register sweep: Pf and X⁻¹
+    within the oracle bounds in FP64, within 1e-3 in FP32; a rank-deficient plane in the
+    batch (rank 2, and a plane with one zero row and column) reports its status and Pf 0
+    without disturbing its neighbours; the result equals the two-barrier tiles' within
+    rounding."""
+    m = mvmc()
+    planes = 300
+    x = skew_batch(np.random.default_rng(100 + n), n, planes)
+    x[7] = 0.0
+    x[7, 0, 1], x[7, 1, 0] = 1.0, -1.0
+    x[11, 5, :] = 0.0
+    x[11, :, 5] = 0.0
+    xc = colmajor(x)
+    ok = np.ones(planes, bool)
+    ok[[7, 11]] = False
+    pf, inv, st = m.pfinv_batch(xc, n, planes)
+    opf, oinv, ost = ol.pfinv_batch(xc, n, planes)
+    assert st[7] > 0 and st[11] > 0 and pf[7] == 0.0 and pf[11] == 0.0
+    assert (st[ok] == 0).all() and (ost[ok] == 0).all()
+    assert np.all(np.sign(pf[ok]) == np.sign(opf[ok]))
+    assert np.max(np.abs(pf[ok] - opf[ok]) / np.abs(opf[ok])) < 1e-12 * max(1, n / 16)
+    inv = inv.reshape(planes, n, n)[ok]
+    oinv = oinv.reshape(planes, n, n)[ok]
+    scale = np.abs(oinv).max(axis=(1, 2), keepdims=True)
+    assert np.max(np.abs(inv - oinv) / scale) < 1e-12 * max(1, n / 16)
+    pf32, inv32, st32 = device_uniform(xc, n, planes, 32)
+    assert (st32[ok] == 0).all() and st32[7] > 0 and st32[11] > 0
+    assert np.max(np.abs(pf32[ok] - opf[ok]) / np.abs(opf[ok])) < 1e-3
+    assert np.max(np.abs(inv32.reshape(planes, n, n)[ok] - oinv) / scale) < 1e-3

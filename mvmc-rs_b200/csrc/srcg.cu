@@ -58,16 +58,38 @@ __device__ double block_sum(double v, double* sh) {
   return t;
 }
 
+// Sum of the per-block partials red[0..gridDim) in a fixed order (lane l adds blocks l,
+// l+32, …, then a fixed shuffle tree), computed by warp 0 and broadcast through sh[33]:
+// every block gets the same bits. red must be complete (after a grid barrier).
+__device__ double blocks_total(const double* red, double* sh) {
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int k = threadIdx.x; k < static_cast<int>(gridDim.x); k += 32) t += red[k];
+    t = warp_sum(t);
+    if (threadIdx.x == 0) sh[33] = t;
+  }
+  __syncthreads();
+  const double t = sh[33];
+  __syncthreads();
+  return t;
+}
+
+// Grid-wide sum of one value per thread into slot `red` (gridDim doubles): block sum, one
+// grid barrier, fixed-order total. The slot may be written again only after a later grid
+// barrier that every block passes after reading it.
+__device__ double grid_sum(cgr::grid_group& grid, double v, double* red, double* sh) {
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) red[blockIdx.x] = v;
+  grid.sync();
+  return blocks_total(red, sh);
+}
+
 // Grid-wide deterministic dot: every block gets the same value.
 __device__ double grid_dot(cgr::grid_group& grid, const double* a, const double* b, int n,
                            double* red, double* sh) {
   double v = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v += a[i] * b[i];
-  v = block_sum(v, sh);
-  if (threadIdx.x == 0) red[blockIdx.x] = v;
-  grid.sync();
-  double t = 0.0;
-  for (int k = 0; k < static_cast<int>(gridDim.x); ++k) t += red[k];
+  const double t = grid_sum(grid, v, red, sh);
   grid.sync();
   return t;
 }
@@ -121,13 +143,15 @@ struct RowBatch {
 
 // out = S·v. FP64: Oᵀ(O·v)/Wc − (⟨O⟩·v)⟨O⟩ + shift·diag ⊙ v. Reduced precision (centred,
 // scaled rows): cs ⊙ Olᵀ(Ol·(cs ⊙ v))/Wc + shift·diag ⊙ v.
+// v may be in global or shared memory; out (global) gets S·v; returns v·(S·v), the same in
+// every block. Two grid barriers: after the column partials and after the dot partials.
 template <typename OT, int KC>
-__device__ void sr_apply_rows(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, double* sh,
-                              unsigned char* smem) {
+__device__ double sr_apply_rows(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, double* red,
+                                double* sh, unsigned char* smem) {
   using CT = typename Elem<OT>::CT;
   constexpr int R = RowBatch<KC>::R;
   constexpr bool kLow = !std::is_same<OT, double>::value;
-  CT* vs = reinterpret_cast<CT*>(smem);
+  CT* vs = reinterpret_cast<CT*>(smem + sizeof(double) * static_cast<size_t>(a.na));
   const int tid = threadIdx.x, nt = blockDim.x, na = a.na;
   for (int i = tid; i < na; i += nt) vs[i] = kLow ? static_cast<CT>(a.cs[i] * v[i]) : static_cast<CT>(v[i]);
   __syncthreads();
@@ -146,32 +170,43 @@ __device__ void sr_apply_rows(cgr::grid_group& grid, const CgArgs& a, const doub
 #pragma unroll
   for (int k = 0; k < KC; ++k) z[k] = 0.0;
   if constexpr (R == 1) {
-    // wide rows: four rows per block sum, the rows read twice (their second read hits L1:
-    // 4 rows of at most 8192 FP64 columns), so a product costs a quarter of the barriers
-    constexpr int R2 = 4;
-    for (long long sb = s0; sb < s1; sb += R2) {
-      double y[R2];
+    // wide rows: chunks of one row per warp; each warp forms y_s = O_s·v of its row with a
+    // shuffle sum (no block barrier per row), then every thread adds y_s·O_s of the chunk's
+    // rows to its columns (the second read of a row comes from L2). One block barrier per
+    // chunk; the chunk's y values are double-buffered.
+    __shared__ double ych[2][kCgThreads / 32];
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    int buf = 0;
+    for (long long sb = s0; sb < s1; sb += nw, buf ^= 1) {
+      const long long s = sb + warp;
+      if (s < s1) {
+        const OT* row = O + s * lda;
+        // sixteen loads in flight per lane: the row streams from memory at full rate
+        constexpr int U = 16;
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        int i = lane;
+        for (; i + 32 * (U - 1) < na; i += 32 * U) {
+          CT x[U];
 #pragma unroll
-      for (int r = 0; r < R2; ++r) y[r] = 0.0;
+          for (int u = 0; u < U; ++u) x[u] = Elem<OT>::load(row + i + 32 * u);
 #pragma unroll
-      for (int k = 0; k < KC; ++k) {
-        const int i = tid + k * nt;
-        if (i >= na) continue;
-        const CT vi = vs[i];
-        CT t[R2];
-#pragma unroll
-        for (int r = 0; r < R2; ++r) t[r] = sb + r < s1 ? Elem<OT>::load(O + (sb + r) * lda + i) : CT(0);
-#pragma unroll
-        for (int r = 0; r < R2; ++r) y[r] += static_cast<double>(t[r] * vi);
+          for (int u = 0; u < U; ++u) t[u & 3] += static_cast<double>(x[u] * vs[i + 32 * u]);
+        }
+        for (; i < na; i += 32) t[0] += static_cast<double>(Elem<OT>::load(row + i) * vs[i]);
+        const double y = warp_sum((t[0] + t[1]) + (t[2] + t[3]));
+        if (lane == 0) ych[buf][warp] = y;
       }
-      block_sum_vec<R2>(y, sh);
+      __syncthreads();
+      const int rows = static_cast<int>(min(static_cast<long long>(nw), s1 - sb));
+#pragma unroll 2
+      for (int r = 0; r < rows; ++r) {
+        const double yv = ych[buf][r];
+        const OT* row = O + (sb + r) * lda;
 #pragma unroll
-      for (int k = 0; k < KC; ++k) {
-        const int i = tid + k * nt;
-        if (i >= na) continue;
-#pragma unroll
-        for (int r = 0; r < R2; ++r)
-          if (sb + r < s1) z[k] += static_cast<double>(Elem<OT>::load(O + (sb + r) * lda + i)) * y[r];
+        for (int k = 0; k < KC; ++k) {
+          const int i = tid + k * nt;
+          if (i < na) z[k] += static_cast<double>(Elem<OT>::load(row + i)) * yv;
+        }
       }
     }
   } else
@@ -211,21 +246,40 @@ __device__ void sr_apply_rows(cgr::grid_group& grid, const CgArgs& a, const doub
     if (i < na) part[i] = z[k];
   }
   grid.sync();
-  for (int i = blockIdx.x * nt + tid; i < na; i += gridDim.x * nt) {
+  // Column totals over the blocks: tiles of 64 columns, each column's block partials split
+  // over nt/64 threads (loads in flight together), the sub-sums added in order.
+  __shared__ double ssub[kCgThreads];
+  const int nsub = nt / 64, nb = static_cast<int>(gridDim.x), bper = (nb + nsub - 1) / nsub;
+  const int cl = tid & 63, sub = tid >> 6, b0 = sub * bper, b1 = min(nb, b0 + bper);
+  double dot = 0.0;
+  for (int tile = blockIdx.x; tile * 64 < na; tile += gridDim.x) {
+    const int col = tile * 64 + cl;
     double t = 0.0;
-    for (int b = 0; b < static_cast<int>(gridDim.x); ++b) t += a.part[static_cast<long long>(b) * na + i];
-    out[i] = kLow ? a.inv_w * (a.cs[i] * t) + a.shift * a.diag[i] * v[i]
-                  : a.inv_w * t - coef * a.mean[i] + a.shift * a.diag[i] * v[i];
+    if (col < na) {
+#pragma unroll 4
+      for (int b = b0; b < b1; ++b) t += a.part[static_cast<long long>(b) * na + col];
+    }
+    ssub[sub * 64 + cl] = t;
+    __syncthreads();
+    if (tid < 64 && col < na) {
+      double tot = 0.0;
+      for (int u = 0; u < nsub; ++u) tot += ssub[u * 64 + tid];
+      const double o = kLow ? a.inv_w * (a.cs[col] * tot) + a.shift * a.diag[col] * v[col]
+                            : a.inv_w * tot - coef * a.mean[col] + a.shift * a.diag[col] * v[col];
+      out[col] = o;
+      dot += v[col] * o;
+    }
+    __syncthreads();
   }
-  grid.sync();
+  return grid_sum(grid, dot, red, sh);
 }
 
 template <typename OT, int KC>
 struct ApplyRows {
   double* sh;
   unsigned char* smem;
-  __device__ void operator()(cgr::grid_group& g, const CgArgs& a, const double* v, double* out) const {
-    sr_apply_rows<OT, KC>(g, a, v, out, sh, smem);
+  __device__ double operator()(cgr::grid_group& g, const CgArgs& a, const double* v, double* out, double* red) const {
+    return sr_apply_rows<OT, KC>(g, a, v, out, red, sh, smem);
   }
 };
 
@@ -235,12 +289,18 @@ __device__ __forceinline__ double precond(const CgArgs& a, int i, double r) {
   return r / dq;
 }
 
-// The C recurrence around an S·v product (apply).
+// The C recurrence around an S·v product (apply), three grid barriers per iteration: the
+// product's column partials, its dot d·(S·d) with the product itself, and the residual
+// update with the new δ. Every block keeps the whole direction d in shared memory (dsh) and
+// forms the next one itself from the published residual, so d is never exchanged; x, r and
+// the preconditioned residual (kept in q) are updated by their owning threads.
 template <typename Apply>
-__device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, const Apply& apply) {
-  const int n = a.na;
+__device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, double* dsh, const Apply& apply) {
+  const int n = a.na, tid = threadIdx.x, nt = blockDim.x;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
   const double threshold = a.tol * a.tol * static_cast<double>(n) * static_cast<double>(n);
+  double* red0 = a.red;               // slot of the product's dot
+  double* red1 = a.red + gridDim.x;   // slot of δ
   double delta;
   for (int i = gtid; i < n; i += gstride) {
     a.x[i] = 0.0;
@@ -248,18 +308,19 @@ __device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, const
   }
   grid.sync();
   if (a.diag_scale) {
-    apply(grid, a, a.x, a.r);
+    apply(grid, a, a.x, a.q, red0);
     for (int i = gtid; i < n; i += gstride) {
-      a.r[i] = a.g[i] - a.r[i];
-      a.d[i] = precond(a, i, a.r[i]);
+      a.r[i] = a.g[i] - a.q[i];
+      a.q[i] = precond(a, i, a.r[i]);
     }
     grid.sync();
-    delta = grid_dot(grid, a.r, a.d, n, a.red, sh);
+    delta = grid_dot(grid, a.r, a.q, n, a.red, sh);
   } else {
-    for (int i = gtid; i < n; i += gstride) a.d[i] = a.g[i];
-    grid.sync();
     delta = grid_dot(grid, a.r, a.r, n, a.red, sh);
   }
+  const double* zsrc = a.diag_scale ? a.q : a.r;
+  for (int i = tid; i < n; i += nt) dsh[i] = zsrc[i];
+  __syncthreads();
   long long status = 0;
   int iter = 0;
   bool done = false;
@@ -271,39 +332,41 @@ __device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, const
     const long long failed = -(static_cast<long long>(iter) + 1);
     if (!isfinite(delta)) { status = failed; done = true; break; }
     if (fabs(delta) < threshold) break;
-    apply(grid, a, a.d, a.q);
-    const double dq = grid_dot(grid, a.d, a.q, n, a.red, sh);
+    const double dq = apply(grid, a, dsh, a.q, red0);
     if (!isfinite(dq) || fabs(dq) < 1e-20) { status = failed; done = true; break; }
     const double alpha = delta / dq;
     if (!isfinite(alpha)) { status = failed; done = true; break; }
-    for (int i = gtid; i < n; i += gstride) a.x[i] += alpha * a.d[i];
-    grid.sync();
-    if ((iter + 1) % 20 == 0) {
-      apply(grid, a, a.x, a.r);
-      for (int i = gtid; i < n; i += gstride) a.r[i] = a.g[i] - a.r[i];
-    } else {
-      for (int i = gtid; i < n; i += gstride) a.r[i] -= alpha * a.q[i];
+    const bool refresh = (iter + 1) % 20 == 0;
+    double part = 0.0;
+    for (int i = gtid; i < n; i += gstride) {
+      a.x[i] += alpha * dsh[i];
+      if (!refresh) {
+        const double ri = a.r[i] - alpha * a.q[i];
+        a.r[i] = ri;
+        const double zi = a.diag_scale ? precond(a, i, ri) : ri;
+        if (a.diag_scale) a.q[i] = zi;
+        part += ri * zi;
+      }
     }
-    grid.sync();
-    double delta_new;
-    if (a.diag_scale) {
-      for (int i = gtid; i < n; i += gstride) a.q[i] = precond(a, i, a.r[i]);
-      grid.sync();
-      delta_new = grid_dot(grid, a.r, a.q, n, a.red, sh);
-    } else {
-      delta_new = grid_dot(grid, a.r, a.r, n, a.red, sh);
+    if (refresh) {
+      grid.sync();  // x complete
+      apply(grid, a, a.x, a.q, red0);
+      for (int i = gtid; i < n; i += gstride) {
+        const double ri = a.g[i] - a.q[i];
+        a.r[i] = ri;
+        const double zi = a.diag_scale ? precond(a, i, ri) : ri;
+        if (a.diag_scale) a.q[i] = zi;
+        part += ri * zi;
+      }
     }
+    const double delta_new = grid_sum(grid, part, red1, sh);
     if (!isfinite(delta_new) || fabs(delta) < 1e-20) { status = failed; done = true; break; }
     const double beta = delta_new / delta;
     if (!isfinite(beta)) { status = failed; done = true; break; }
-    if (a.diag_scale) {
-      delta = delta_new;
-      for (int i = gtid; i < n; i += gstride) a.d[i] = a.q[i] + beta * a.d[i];
-    } else {
-      delta *= beta;
-      for (int i = gtid; i < n; i += gstride) a.d[i] = a.r[i] + beta * a.d[i];
-    }
-    grid.sync();
+    if (a.diag_scale) delta = delta_new;
+    else delta *= beta;
+    for (int i = tid; i < n; i += nt) dsh[i] = zsrc[i] + beta * dsh[i];
+    __syncthreads();
     ++iter;
   }
   if (!done) {
@@ -321,34 +384,44 @@ __device__ void cg_run(cgr::grid_group& grid, const CgArgs& a, double* sh, const
 // Gram form (o_kind 3): out = Wc⁻¹·cs ⊙ (G·(cs ⊙ v)) + shift·diag ⊙ v with G = ÕᵀÕ formed once
 // on the tensor cores (FP32, na × na, row stride lda). One warp per row of G (FP64
 // accumulation, lanes then shuffles in a fixed order), rows strided over the grid.
-__device__ void sr_apply_gram(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, unsigned char* smem) {
-  double* u = reinterpret_cast<double*>(smem);
+__device__ double sr_apply_gram(cgr::grid_group& grid, const CgArgs& a, const double* v, double* out, double* red,
+                                double* sh, unsigned char* smem) {
+  double* u = reinterpret_cast<double*>(smem + sizeof(double) * static_cast<size_t>(a.na));
   const int tid = threadIdx.x, nt = blockDim.x, na = a.na, lane = tid & 31;
   for (int i = tid; i < na; i += nt) u[i] = a.cs[i] * v[i];
   __syncthreads();
   const float* G = static_cast<const float*>(a.Ol);
   const int gw = (blockIdx.x * nt + tid) >> 5, nw = (gridDim.x * nt) >> 5;
+  double dot = 0.0;
   for (int i = gw; i < na; i += nw) {
     const float* row = G + static_cast<long long>(i) * a.lda;
-    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    // sixteen loads in flight per lane (G is read from L2)
+    constexpr int U = 16;
+    double tt[4] = {0.0, 0.0, 0.0, 0.0};
     int j = lane;
-    for (; j + 96 < na; j += 128) {
-      t0 += static_cast<double>(__ldg(row + j)) * u[j];
-      t1 += static_cast<double>(__ldg(row + j + 32)) * u[j + 32];
-      t2 += static_cast<double>(__ldg(row + j + 64)) * u[j + 64];
-      t3 += static_cast<double>(__ldg(row + j + 96)) * u[j + 96];
+    for (; j + 32 * (U - 1) < na; j += 32 * U) {
+      float g[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) g[k] = __ldg(row + j + 32 * k);
+#pragma unroll
+      for (int k = 0; k < U; ++k) tt[k & 3] += static_cast<double>(g[k]) * u[j + 32 * k];
     }
-    for (; j < na; j += 32) t0 += static_cast<double>(__ldg(row + j)) * u[j];
-    const double t = warp_sum((t0 + t1) + (t2 + t3));
-    if (lane == 0) out[i] = a.inv_w * (a.cs[i] * t) + a.shift * a.diag[i] * v[i];
+    for (; j < na; j += 32) tt[0] += static_cast<double>(__ldg(row + j)) * u[j];
+    const double t = warp_sum((tt[0] + tt[1]) + (tt[2] + tt[3]));
+    if (lane == 0) {
+      const double o = a.inv_w * (a.cs[i] * t) + a.shift * a.diag[i] * v[i];
+      out[i] = o;
+      dot += v[i] * o;
+    }
   }
-  grid.sync();
+  return grid_sum(grid, dot, red, sh);
 }
 
 struct ApplyGram {
+  double* sh;
   unsigned char* smem;
-  __device__ void operator()(cgr::grid_group& g, const CgArgs& a, const double* v, double* out) const {
-    sr_apply_gram(g, a, v, out, smem);
+  __device__ double operator()(cgr::grid_group& g, const CgArgs& a, const double* v, double* out, double* red) const {
+    return sr_apply_gram(g, a, v, out, red, sh, smem);
   }
 };
 
@@ -356,7 +429,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_sr_cg_gram(CgArgs a) {
   cgr::grid_group grid = cgr::this_grid();
   __shared__ double sh[32 * 8 + 8 + 8];
   extern __shared__ __align__(16) unsigned char smem[];
-  cg_run(grid, a, sh, ApplyGram{smem});
+  cg_run(grid, a, sh, reinterpret_cast<double*>(smem), ApplyGram{sh, smem});
 }
 
 template <typename OT, int KC>
@@ -372,7 +445,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_sr_cg(CgArgs a) {
     }
     return;
   }
-  cg_run(grid, a, sh, ApplyRows<OT, KC>{sh, smem});
+  cg_run(grid, a, sh, reinterpret_cast<double*>(smem), ApplyRows<OT, KC>{sh, smem});
 }
 
 // Gather the active columns of the stored O rows: Oa[s][si] = store[s][map[si] + 1].
@@ -524,7 +597,8 @@ int launch_gather_active_low(const double* store, int sr_size, long long ns, con
 template <typename OT, int KC>
 int launch_cg_kc(CgArgs& a, cudaStream_t stream) {
   void* args[] = {&a};
-  const size_t smem = sizeof(typename Elem<OT>::CT) * static_cast<size_t>(a.na);
+  // the direction d (FP64) and the staged product input (element type)
+  const size_t smem = (sizeof(double) + sizeof(typename Elem<OT>::CT)) * static_cast<size_t>(a.na);
   auto kernel = k_sr_cg<OT, KC>;
   MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kernel), cg_grid_blocks(a.ns, a.na), kCgThreads,
@@ -547,7 +621,7 @@ int launch_cg_type(CgArgs& a, cudaStream_t stream) {
 int launch_sr_cg(CgArgs a, cudaStream_t stream) {
   if (a.o_kind == 3) {  // Gram form: G (FP32) in a.Ol, no sample pass per iteration
     void* args[] = {&a};
-    const size_t smem = sizeof(double) * static_cast<size_t>(a.na);
+    const size_t smem = 2 * sizeof(double) * static_cast<size_t>(a.na);
     MVMCB_CUDA(cudaFuncSetAttribute(k_sr_cg_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     MVMCB_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_sr_cg_gram), cg_grid_blocks(a.ns, a.na),
                                            kCgThreads, args, smem, stream));

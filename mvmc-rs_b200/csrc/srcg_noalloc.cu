@@ -11,7 +11,7 @@
 // The array holds kNoAllocScratchDoubles doubles (8 MiB) on every GPU that loads the
 // library, for the lifetime of the process. A solve needs
 //   3·na (residual, direction, product) + ns (row products)
-//   + nchunk·na (column partial sums) + blocks (block partials)
+//   + nchunk·na (column partial sums) + 2·blocks (two slots of block partials)
 // doubles of it; larger problems are rejected with MVMC_B200_EARG and a message.
 // Every call uses the same array: calls that overlap on the GPU (two streams, or two
 // host threads on one device) race on it and must be serialised by the caller. Each
@@ -86,7 +86,7 @@ extern "C" int mvmc_b200_cg_solve_noalloc(const double* samples, long long ns, i
   }
   const int blocks = cg_grid_blocks(ns, na);
   const int nchunk = cg_nchunk(ns, na, 0, blocks);
-  const long long need = 3LL * na + ns + static_cast<long long>(nchunk) * na + blocks;
+  const long long need = 3LL * na + ns + static_cast<long long>(nchunk) * na + 2LL * blocks;
   if (need > kNoAllocScratchDoubles) {
     set_last_error("cg_solve_noalloc: problem needs " + std::to_string(need) +
                    " scratch doubles; the array holds 1048576 (8 MiB)");

@@ -72,7 +72,7 @@ enum Ctl {
   cSkip = 0, cType, cMi, cRi, cRj, cS, cMj, cT, cMsa, cMsb, cAccept, cRefresh, cInfo, cNacc,
   cBurn, cAttempt, cStop
 };
-enum DCtl { dLogIp = 0, dLogIpNew = 1, dDproj = 2 };
+enum DCtl { dLogIp = 0, dLogIpNew = 1, dDproj = 2, dRefreshMask = 3 };
 
 template <typename T>
 struct WalkerSmem {
@@ -192,8 +192,11 @@ __device__ void make_proj_cnt_cta(const DevModel& m, const int* jtab, const int*
 // shared memory when they are there (the plane is gathered into the first buffer and the
 // result copied to the plane), else in place on an FP64 plane in L2 (rows p, q of each
 // pivot step snapshot in the shared GJ rows).
+// mask: the planes to recompute (bit q; planes from 64 on always); the others keep their
+// Pf and inverse.
 template <typename T, int JPL, bool kSmemPlanes, bool kSmemWs>
-__device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status) {
+__device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigned* status,
+                              unsigned long long mask = ~0ull) {
   const int n = m.n;
   constexpr bool kFp64Planes = sizeof(T) == sizeof(double);
   // in place: FP64 planes in shared memory, or FP64 planes in L2 without shared buffers
@@ -202,6 +205,7 @@ __device__ int calc_m_all_dev(const DevModel& m, const WalkerSmem<T>& s, unsigne
   constexpr int RB = kSmemSweep ? 1 : (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1));
   int info = 0;
   for (int q = 0; q < m.nqp; ++q) {
+    if (q < 64 && !((mask >> q) & 1ull)) continue;
     T* P = s.planes + static_cast<size_t>(q) * n * n;
     double* A = kInPlace ? reinterpret_cast<double*>(P) : s.ws;
     double* B = kInPlace ? s.ws : s.ws2;
@@ -932,7 +936,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
         if (!isfinite(wgt)) wgt = -1.0;
         const double u = rng.real2();
         const int acc = wgt > u ? 1 : 0;
-        int guard = 0;
+        unsigned long long guard = 0ull;  // planes whose ratio tripped the guard
         if (acc) {
           s.dctl[dLogIp] = lip_new;
           ++n_acc_win;
@@ -943,7 +947,7 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
             // the rank-2 update amplifies the inverse's rounding error by about 1/|ratio|
             for (int q = 0; q < m.nqp; ++q) {
               const double r = fabs(s.pfn[q] / s.pf[q]);
-              if (!(r >= w.refresh_guard && r * w.refresh_guard <= 1.0)) guard = 1;
+              if (!(r >= w.refresh_guard && r * w.refresh_guard <= 1.0)) guard |= q < 64 ? (1ull << q) : ~0ull;
             }
           }
         } else if (type == 0) {
@@ -962,11 +966,12 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
           n_acc_win = 0;
         }
         if (guard && !refresh) refresh = 3;
-        if (refresh) since_refresh = 0;
-        if (refresh == 3) {
-          ++n_guard;
-          n_acc_win = 0;
-        }
+        // a guard refresh recomputes only the planes that tripped it (the others carry no
+        // amplified error); a scheduled one recomputes every plane
+        reinterpret_cast<unsigned long long*>(s.dctl)[dRefreshMask] = refresh == 3 ? guard : ~0ull;
+        // the schedules (accept window, NRefresh) restart only at a refresh of every plane
+        if (refresh == 1 || refresh == 2) since_refresh = 0;
+        if (refresh == 3) ++n_guard;
         else if (refresh) ++n_sched;
         cc[cRefresh] = refresh;
       }
@@ -981,7 +986,8 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
       }
       lap(kPhUpdate);
       if (cc[cRefresh]) {
-        const int info = calc_m_all_dev<T, JPL, kSmemPlanes, kSmemWs>(m, s, w.status);
+        const unsigned long long rmask = reinterpret_cast<const unsigned long long*>(s.dctl)[dRefreshMask];
+        const int info = calc_m_all_dev<T, JPL, kSmemPlanes, kSmemWs>(m, s, w.status, rmask);
         if (tid == 0 && info == 0) {
           // drift of the incrementally updated amplitude against the FP64 recomputation
           const double fresh = log_ip_of(m, s.pf, s.qpw);

@@ -46,7 +46,7 @@ METRIC = "Metropolis sweeps/s & SR-step time: mixed vs FP64 path on 1 B200 at |d
 # DRAM bytes (read + write) per walker-sweep of k_sample from an ncu capture of a small
 # case of the same kernel instance (profiles/k_sample_fp64_square8_w296.txt: 2.594 GB over
 # 296 walkers x 4 sweeps), scaled to a launch by walker-sweeps.
-SAMPLE_DRAM_PER_WALKER_SWEEP = {("square8", 64): 2.594e9 / (296 * 4)}
+SAMPLE_DRAM_PER_WALKER_SWEEP = {("square8", 64): 2.607e9 / (296 * 4)}
 PFINV_METRIC = "Pfaffian+inverse/s (batched skew FP64)"
 PHYSCAL = {"physcal8": 4096}
 PHYSCAL_METRIC = "PhysCal samples/s (energy + one- and two-body Green functions, FP64)"

@@ -1077,8 +1077,14 @@ int launch_sample_t(const DevModel& m, const DevWalkers& w, cudaStream_t stream)
 // Shared-memory residency: planes (and for FP32 the FP64 refresh workspace) in shared
 // memory when they fit the per-block opt-in limit.
 int residency_policy();
+// FP32 planes: several small QP planes (side ≤ 64) go to L2 with two walkers per SM, which
+// overlap each other's serial phases (2D 8×8, eight planes of 64: 2.08 against 2.63 s per
+// SR step with one walker per SM holding its planes in shared memory); one wide plane stays
+// in shared memory (2D 16×16: 68.7 against 84.2 ms in L2).
+bool fp32_prefers_l2(const DevModel& m) { return residency_policy() == 0 && m.nqp >= 4 && m.n <= 64; }
 bool sample_planes_in_smem(const DevModel& m, int precision, int limit) {
   if (residency_policy() == 1) return false;
+  if (precision == 32 && fp32_prefers_l2(m)) return false;
   if (precision == 32) return samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit) ||
                               samp_layout<float>(m, true, false).total <= static_cast<size_t>(limit);
   return samp_layout<double>(m, true, true).total <= static_cast<size_t>(limit);
@@ -1157,6 +1163,7 @@ int launch_sample_jpl(const DevModel& m, const DevWalkers& w, int precision, int
     if (precision == 32) return launch_sample_global<float, JPL>(m, w, stream);
     return launch_sample_global<double, JPL>(m, w, stream);
   }
+  if (precision == 32 && fp32_prefers_l2(m)) return launch_sample_global<float, JPL>(m, w, stream);
   if (precision == 32) {
     if (samp_layout<float>(m, true, true).total <= static_cast<size_t>(limit)) {
       if constexpr (JPL == 1) {

@@ -52,6 +52,8 @@ int launch_gather_active_low(const double* store, int sr_size, long long ns, con
 int launch_stage(const DevModel& m, const StageBufs& b, int op, int msa, int msb, int rsa_old, int rsb_old,
                  unsigned* status, cudaStream_t stream);
 int launch_gram(const double* store, int n, long long ns, double inv_w, double* oo, cudaStream_t stream);
+int launch_assemble_s_gram(const float* g, int ldg, const double* cs, const double* var, int na, double inv_wc,
+                           double sta_del, double* s, cudaStream_t stream);
 int launch_assemble_s(const double* oo, int n, const int* map, int na, double ratio_diag, double* s,
                       cudaStream_t stream);
 int launch_cholesky_solve(double* a, int n, double* b, int* info_dev, cudaStream_t stream);
@@ -614,22 +616,32 @@ int do_sr_direct(mvmc_b200_ctx* c, double* info_out) {
   const double wc = c->tot[0];
   const double* ho = c->tot.data() + 5;
   const long long ns = static_cast<long long>(c->W) * c->S;
-  const size_t nn = static_cast<size_t>(size) * size;
-  if (nn > c->oo_cap) {
-    c->d_oo = c->alloc<double>(nn);
-    c->oo_cap = nn;
-  }
   if (!c->d_info) c->d_info = c->alloc<int>(1);
-  int rc = launch_gram(c->d_ostore, size, ns, 1.0 / wc, c->d_oo, c->stream);
-  if (rc != kOk) return rc;
-  // row 0 (⟨O⟩) and the diagonal (⟨O²⟩) of OO for the redundancy cut and g
+  // sr_precision 16 / 32: the active S block from the tensor-core Gram of the centred,
+  // column-scaled samples (BF16 / TF32 inputs, FP32 accumulation), ⟨O⟩ and ⟨O²⟩ from the
+  // measurement sums; otherwise the FP64 Gram of every O column (the C order)
+  const bool tc = !c->opt.c_order && (c->opt.sr_precision == 16 || c->opt.sr_precision == 32);
+  int rc = kOk;
   std::vector<double> row0(size), diag(size);
-  check(cudaMemcpyAsync(row0.data(), c->d_oo, sizeof(double) * size, cudaMemcpyDeviceToHost, c->stream), "OO row 0");
-  check(cudaMemcpy2DAsync(diag.data(), sizeof(double), c->d_oo, sizeof(double) * (size + 1), sizeof(double), size,
-                          cudaMemcpyDeviceToHost, c->stream),
-        "OO diagonal");
-  check(cudaStreamSynchronize(c->stream), "gram");
-  c->d2h += static_cast<long long>(sizeof(double) * 2 * size);
+  if (tc) {
+    std::copy(c->tot.begin() + 5 + size, c->tot.begin() + 5 + 2 * size, row0.begin());
+    std::copy(c->tot.begin() + 5 + 2 * size, c->tot.begin() + 5 + 3 * size, diag.begin());
+  } else {
+    const size_t nn = static_cast<size_t>(size) * size;
+    if (nn > c->oo_cap) {
+      c->d_oo = c->alloc<double>(nn);
+      c->oo_cap = nn;
+    }
+    rc = launch_gram(c->d_ostore, size, ns, 1.0 / wc, c->d_oo, c->stream);
+    if (rc != kOk) return rc;
+    // row 0 (⟨O⟩) and the diagonal (⟨O²⟩) of OO for the redundancy cut and g
+    check(cudaMemcpyAsync(row0.data(), c->d_oo, sizeof(double) * size, cudaMemcpyDeviceToHost, c->stream), "OO row 0");
+    check(cudaMemcpy2DAsync(diag.data(), sizeof(double), c->d_oo, sizeof(double) * (size + 1), sizeof(double), size,
+                            cudaMemcpyDeviceToHost, c->stream),
+          "OO diagonal");
+    check(cudaStreamSynchronize(c->stream), "gram");
+    c->d2h += static_cast<long long>(sizeof(double) * 2 * size);
+  }
   std::vector<double> s_diag(npara);
   for (int pi = 0; pi < npara; ++pi) s_diag[pi] = diag[pi + 1] - row0[pi + 1] * row0[pi + 1];
   bool any_nan = false;
@@ -668,7 +680,48 @@ int do_sr_direct(mvmc_b200_ctx* c, double* info_out) {
   check(cudaMemcpyAsync(c->d_map, map.data(), sizeof(int) * na, cudaMemcpyHostToDevice, c->stream), "upload map");
   check(cudaMemcpyAsync(d_g, g.data(), sizeof(double) * na, cudaMemcpyHostToDevice, c->stream), "upload g");
   c->h2d += static_cast<long long>(sizeof(int) * na + sizeof(double) * na);
-  rc = launch_assemble_s(c->d_oo, size, c->d_map, na, 1.0 + m.sta_del, d_s, c->stream);
+  if (tc) {
+    // active ⟨O⟩, variance and column scales (the standard deviations) for the staging
+    const int prec = c->opt.sr_precision;
+    if (static_cast<size_t>(8) * na > c->cgvec_cap) {
+      c->d_cgvec = c->alloc<double>(static_cast<size_t>(8) * na);
+      c->cgvec_cap = static_cast<size_t>(8) * na;
+    }
+    std::vector<double> v3(static_cast<size_t>(3) * na);
+    for (int si = 0; si < na; ++si) {
+      const double var = s_diag[map[si]];
+      v3[si] = row0[map[si] + 1];
+      v3[na + si] = var;
+      v3[2 * na + si] = (std::isfinite(var) && var > 0.0) ? std::sqrt(var) : 1.0;
+    }
+    double* d_mean = c->d_cgvec;
+    double* d_var = c->d_cgvec + na;
+    double* d_cs = c->d_cgvec + 7 * static_cast<size_t>(na);
+    check(cudaMemcpyAsync(d_mean, v3.data(), sizeof(double) * 2 * na, cudaMemcpyHostToDevice, c->stream),
+          "upload mean, var");
+    check(cudaMemcpyAsync(d_cs, v3.data() + 2 * na, sizeof(double) * na, cudaMemcpyHostToDevice, c->stream),
+          "upload column scales");
+    c->h2d += static_cast<long long>(sizeof(double) * 3 * na);
+    int na_pad = 0;
+    long long ld = 0;
+    gram_tc_dims(na, ns, prec, &na_pad, &ld);
+    const size_t staged = static_cast<size_t>(na_pad) * ld * (prec == 16 ? 2 : 4);
+    if (staged > c->staged_cap) {
+      c->d_staged = c->alloc<unsigned char>(staged);
+      c->staged_cap = staged;
+    }
+    if (static_cast<size_t>(na) * na > c->gram_cap) {
+      c->d_gram = c->alloc<float>(static_cast<size_t>(na) * na);
+      c->gram_cap = static_cast<size_t>(na) * na;
+    }
+    rc = launch_gram_stage(c->d_ostore, size, ns, c->d_map, na, d_mean, d_cs, prec, c->d_staged, c->stream);
+    if (rc != kOk) return rc;
+    rc = launch_gram_tc(c->d_staged, na, ns, prec, c->d_gram, na, c->dw.status, c->stream);
+    if (rc != kOk) return rc;
+    rc = launch_assemble_s_gram(c->d_gram, na, d_cs, d_var, na, 1.0 / wc, m.sta_del, d_s, c->stream);
+  } else {
+    rc = launch_assemble_s(c->d_oo, size, c->d_map, na, 1.0 + m.sta_del, d_s, c->stream);
+  }
   if (rc != kOk) return rc;
   rc = launch_cholesky_solve(d_s, na, d_g, c->d_info, c->stream);
   if (rc != kOk) return rc;
@@ -677,6 +730,11 @@ int do_sr_direct(mvmc_b200_ctx* c, double* info_out) {
   check(cudaMemcpyAsync(g.data(), d_g, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream), "download x");
   check(cudaStreamSynchronize(c->stream), "sr-direct");
   c->d2h += static_cast<long long>(sizeof(double) * na + sizeof(int));
+  if (tc) {
+    unsigned dst = 0;
+    check(cudaMemcpy(&dst, c->dw.status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+    if (dst & kDevTimeout) throw std::runtime_error("sr-direct: the tensor-core Gram timed out (cuda device wait)");
+  }
   if (info != 0) return 1;
   for (double v : g)
     if (!std::isfinite(v)) return 1;

@@ -103,6 +103,22 @@ __global__ void k_assemble_s(const double* __restrict__ oo, int n, const int* __
   }
 }
 
+// S of the active block from the tensor-core Gram of the centred, column-scaled samples
+// (G = ÕᵀÕ, FP32, row stride ldg): S_ij = Wc⁻¹·cs_i·G_ij·cs_j, plus sta_del·var_i on the
+// diagonal (the same operator the Gram form of SR-CG applies), in FP64.
+__global__ void k_assemble_s_gram(const float* __restrict__ g, int ldg, const double* __restrict__ cs,
+                                  const double* __restrict__ var, int na, double inv_wc, double sta_del,
+                                  double* __restrict__ s) {
+  const long long total = static_cast<long long>(na) * na;
+  for (long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; k < total;
+       k += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(k / na), j = static_cast<int>(k - static_cast<long long>(i) * na);
+    double v = inv_wc * (cs[i] * static_cast<double>(g[static_cast<size_t>(i) * ldg + j]) * cs[j]);
+    if (i == j) v += sta_del * var[i];
+    s[k] = v;
+  }
+}
+
 // In-place lower Cholesky of the row-major n×n matrix a (the lower triangle is read and
 // written). info: 0, or the 1-based row of the first non-positive / non-finite pivot.
 __global__ void __launch_bounds__(kCholThreads) k_cholesky(double* __restrict__ a, int n, int* info) {
@@ -273,6 +289,15 @@ int launch_assemble_s(const double* oo, int n, const int* map, int na, double ra
   const long long total = static_cast<long long>(na) * na;
   const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16)));
   k_assemble_s<<<grid, 256, 0, stream>>>(oo, n, map, na, ratio_diag, s);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
+int launch_assemble_s_gram(const float* g, int ldg, const double* cs, const double* var, int na, double inv_wc,
+                           double sta_del, double* s, cudaStream_t stream) {
+  const long long total = static_cast<long long>(na) * na;
+  const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16)));
+  k_assemble_s_gram<<<grid, 256, 0, stream>>>(g, ldg, cs, var, na, inv_wc, sta_del, s);
   MVMCB_CUDA(cudaGetLastError());
   return kOk;
 }

@@ -78,3 +78,34 @@ def test_direct_sr_optimisation_matches_oracle(tmp_path, case):
     vb = read_out(odir / "zvo_var.dat")
     scale = np.abs(vb).max(axis=1, keepdims=True)
     assert np.all(np.abs(va - vb) <= 1e-6 * scale)
+
+
+@pytest.mark.parametrize("sr_precision,bound", [(32, 1e-2), (16, 5e-2)])
+def test_direct_sr_through_tensor_core_gram(tmp_path, sr_precision, bound):
+    """Direct SR (NSRCG 0) with sr_precision 32 / 16: the active S block from the
+    tensor-core Gram of the centred, column-scaled samples (TF32 / BF16 inputs, FP32
+    accumulation), the Cholesky solve in FP64. On identical samples (FP64 sampling, same
+    seeds) the active set equals the FP64 direct step's and the parameter update is within
+    1e-2 (TF32) / 5e-2 (BF16) relative of it."""
+    lat = lattice()
+    cfg = dict(lat.CONFIGS["square8"])
+    cfg.update(interval=2, nsrcg=0)
+    nl, init, _ = lat.write_inputs(str(tmp_path / "in"), **cfg)
+
+    def update(srp):
+        eng = mvmc().Engine(nl, init, walkers=1024, precision=64, seed=7, sr_precision=srp)
+        p0 = eng.parameters()
+        eng.sample()
+        eng.measure()
+        rc, info = eng.sr_cg()
+        dp = eng.parameters() - p0
+        eng.close()
+        return rc, info, dp
+
+    rc64, info64, d64 = update(64)
+    rc, info, d = update(sr_precision)
+    assert rc == rc64 == 0
+    assert np.array_equal(info[:4], info64[:4]), (info, info64)
+    assert np.linalg.norm(d64) > 0
+    err = np.linalg.norm(d - d64) / np.linalg.norm(d64)
+    assert err <= bound, err

@@ -171,7 +171,7 @@ int mvmc_b200_cg_solve(const double* samples, long long ns, int na, const double
  * mean/diag/g [na] inputs; x [na] and result [3] = {delta, status, iterations} outputs.
  * The working vectors live in an 8 MiB array compiled into the library (held on every
  * GPU that loads it until exit); problems needing more than 1048576 doubles of it
- * (3·na + ns + column partials) return MVMC_B200_EARG with a message. The first call on
+ * (3·na + ns + column and block partials) return MVMC_B200_EARG with a message. The first call on
  * a device looks up that array's device address; make it before any stream capture.
  * Calls share the array: calls that overlap on the GPU race and must be serialised.
  * stream is a cudaStream_t (NULL = default); the call returns once the solve is queued. */

@@ -84,7 +84,9 @@ typedef struct mvmc_b200_options {
   long long seed;       /* < 0: RndSeed of modpara.def */
   int device;           /* CUDA device ordinal */
   int sr_precision;     /* SR-CG sample matrix: 64 (or 0) FP64 in the C order; 32 FP32 or 16 BF16,
-                         * centred and column-scaled, FP32 products (the mixed path's operator) */
+                         * centred and column-scaled, FP32 products (the mixed path's operator).
+                         * Direct SR (NSRCG 0) with 32 / 16 assembles S from the tensor-core Gram
+                         * of those samples (TF32 / BF16 inputs) and solves it in FP64. */
   double refresh_guard; /* g in [0, 1): FP64 refresh right after an accepted move whose Pfaffian
                          * ratio on any QP plane lies outside [g, 1/g]; 0 = off (C behaviour) */
   int c_order;          /* 1: measurement, its sums and SR-CG in the reference CPU path's operation

@@ -11,7 +11,7 @@
 // chunks of 16 rows; every entry is summed in sample order, then mirrored.
 // K7 k_cholesky: one cooperative launch, right-looking with 32-wide panels: block 0
 // factors the diagonal block in shared memory, all blocks solve the panel rows below it,
-// all blocks update the trailing lower triangle in 32×32 tiles (grid barrier between the
+// all blocks update the trailing lower triangle in 64×64 tiles (grid barrier between the
 // three). S = L Lᵀ with L = Uᵀ of dpotrf('U'). K8 k_cholesky_solve: one block, the
 // forward and backward substitutions blocked by 32.
 #include <cooperative_groups.h>
@@ -31,7 +31,8 @@ namespace mvmcb {
 
 constexpr int kGramTile = 64;
 constexpr int kGramK = 16;
-constexpr int kCholB = 32;
+constexpr int kCholB = 32;   // panel width
+constexpr int kCholT = 64;   // trailing-update tile (kCholThreads = 16 × 16 threads, 4 × 4 each)
 constexpr int kCholThreads = 256;
 
 // OO[i][j] (i ≥ j tiles) of the rows store[s][0..n) for s < ns, scaled by inv_w.
@@ -124,8 +125,8 @@ __global__ void k_assemble_s_gram(const float* __restrict__ g, int ldg, const do
 __global__ void __launch_bounds__(kCholThreads) k_cholesky(double* __restrict__ a, int n, int* info) {
   cgr::grid_group grid = cgr::this_grid();
   __shared__ double D[kCholB][kCholB + 1];
-  __shared__ double Li[kCholB][kCholB + 1];
-  __shared__ double Lj[kCholB][kCholB + 1];
+  __shared__ double Ti[kCholT][kCholB + 1];
+  __shared__ double Tj[kCholT][kCholB + 1];
   __shared__ int s_fail;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int k0 = 0; k0 < n; k0 += kCholB) {
@@ -188,31 +189,48 @@ __global__ void __launch_bounds__(kCholThreads) k_cholesky(double* __restrict__ 
         if (j < kb) row[j] = x[j];
     }
     grid.sync();
-    // (3) trailing update of the lower triangle, 32×32 tiles
-    const int m = (rest + kCholB - 1) / kCholB;
+    // (3) trailing update of the lower triangle in 64×64 tiles (4×4 outputs per thread,
+    // the tile's two 64×32 panel slices staged in shared memory)
+    const int m = (rest + kCholT - 1) / kCholT;
     const int ntiles = m * (m + 1) / 2;
+    const int tr = tid / 16, tc = tid % 16;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       int ti = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) / 2.0);
       while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
       while (ti * (ti + 1) / 2 > t) --ti;
       const int tj = t - ti * (ti + 1) / 2;
-      const int i0 = k0 + kb + ti * kCholB, j0 = k0 + kb + tj * kCholB;
-      for (int e = tid; e < kCholB * kCholB; e += nt) {
+      const int i0 = k0 + kb + ti * kCholT, j0 = k0 + kb + tj * kCholT;
+      for (int e = tid; e < kCholT * kCholB; e += nt) {
         const int r = e / kCholB, c = e - r * kCholB;
-        Li[r][c] = (i0 + r < n && c < kb) ? a[static_cast<size_t>(i0 + r) * n + k0 + c] : 0.0;
-        Lj[r][c] = (j0 + r < n && c < kb) ? a[static_cast<size_t>(j0 + r) * n + k0 + c] : 0.0;
+        Ti[r][c] = (i0 + r < n && c < kb) ? a[static_cast<size_t>(i0 + r) * n + k0 + c] : 0.0;
+        Tj[r][c] = (j0 + r < n && c < kb) ? a[static_cast<size_t>(j0 + r) * n + k0 + c] : 0.0;
       }
       __syncthreads();
-      for (int e = tid; e < kCholB * kCholB; e += nt) {
-        const int r = e / kCholB, c = e - r * kCholB;
-        const int i = i0 + r, j = j0 + c;
-        if (i < n && j < n && j <= i) {
-          double t = 0.0;
+      double acc[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
 #pragma unroll 8
-          for (int k = 0; k < kCholB; ++k) t += Li[r][k] * Lj[c][k];
-          a[static_cast<size_t>(i) * n + j] -= t;
+      for (int k = 0; k < kCholB; ++k) {
+        double li[4], lj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          li[u] = Ti[tr + 16 * u][k];
+          lj[u] = Tj[tc + 16 * u][k];
         }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] += li[u] * lj[v];
       }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const int i = i0 + tr + 16 * u, j = j0 + tc + 16 * v;
+          if (i < n && j < n && j <= i) a[static_cast<size_t>(i) * n + j] -= acc[u][v];
+        }
       __syncthreads();
     }
     grid.sync();

@@ -372,7 +372,9 @@ def sr16_record(args, local, timed=3):
     refresh; SR-CG through the tensor-core Gram of the centred, column-scaled samples with
     TF32 inputs), and the mixed path's errors on the first step from the same seeds and
     parameters: energy per site, variance, <O_k> and the SR parameter update; the update
-    error of each reduced-precision SR operator alone on the FP64 path's samples."""
+    error of each reduced-precision SR operator alone on the FP64 path's samples; and the FP64
+    path with the resident measurement (Pf and X⁻¹ of each saved sample as the sampler held
+    them, not recomputed)."""
     import torch
     import lattice
     import mvmc_b200 as mb
@@ -381,11 +383,11 @@ def sr16_record(args, local, timed=3):
     nl, init, dims = lattice.write_inputs(os.path.join(tmp, "in"), **cfg)
     W = WALKERS["square16_sr"]
 
-    def run(precision, sr_precision, steps, sr_gram=0):
+    def run(precision, sr_precision, steps, sr_gram=0, resident=0):
         eng = mb.Engine(nl, init, walkers=W, precision=precision, seed=12345,
                         refresh_sweeps=args.refresh if precision == 32 else 0,
                         refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision,
-                        sr_gram=sr_gram)
+                        sr_gram=sr_gram, measure_resident=resident)
         stream = torch.cuda.ExternalStream(eng.stream())
         p0 = eng.parameters()
         eng.sample()
@@ -416,6 +418,8 @@ def sr16_record(args, local, timed=3):
 
     a_first, a_t = run(64, 64, timed)
     c_first, c_t = run(32, 32, timed, sr_gram=1)
+    # FP64 path whose measurement reads the sampler's resident Pf and X⁻¹
+    r_first, r_t = run(64, 64, timed, resident=1)
     op_err = {}
     for name, srp, gram in (("tf32_gram", 32, 1), ("bf16_gram", 16, 1), ("bf16_gemv", 16, 0)):
         f, _ = run(64, srp, 0, sr_gram=gram)
@@ -428,6 +432,9 @@ def sr16_record(args, local, timed=3):
         "workload": "square16_sr", "walkers": W, "n": dims["n"], "npara": dims["npara"],
         "sweeps_per_walker_step": (cfg["samples"] + 1) * cfg["interval"],
         "fp64": a_t, "mixed": c_t,
+        "fp64_resident_measurement": dict(r_t, dE_per_site_first_step=float(
+            abs(r_first["e"][1] - a_first["e"][1]) / ns), identical_chains_first_step=float(
+            np.mean(np.all(r_first["idx"] == a_first["idx"], axis=1)))),
         "mixed_over_fp64": {"sr_step": a_t["sr_step_ms"] / c_t["sr_step_ms"],
                             "sweeps": a_t["sample_ms"] / c_t["sample_ms"],
                             "measure": a_t["measure_ms"] / c_t["measure_ms"],

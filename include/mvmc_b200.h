@@ -97,6 +97,11 @@ typedef struct mvmc_b200_options {
                          * centred, column-scaled samples, formed once per SR step on the tensor cores
                          * (BF16 / TF32 inputs, FP32 accumulation); 0: one pass over the samples per
                          * CG product */
+  int measure_resident; /* 1 with precision 64: the sampler stores each saved sample's Pf and X⁻¹ as it
+                         * holds them (after its rank-2 / rank-4 updates since the last refresh) and the
+                         * measurement reads them instead of recomputing (the reference recomputes
+                         * them, CalculateMAll per sample); W·saved·NQP·n² doubles of device memory.
+                         * 0: recompute. */
 } mvmc_b200_options;
 
 void mvmc_b200_default_options(mvmc_b200_options* opt);

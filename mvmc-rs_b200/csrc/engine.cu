@@ -506,6 +506,13 @@ void build_context(mvmc_b200_ctx* c, const char* namelist, const char* initial_d
   }
   // FP64 sweep buffers of walkers whose buffers are not in shared memory (two per walker)
   dw.ws64 = c->alloc<double>(static_cast<size_t>(W) * 2 * nn);
+  // resident measurement (FP64 path): the sampler's Pf and X⁻¹ at every save point
+  if (opt.measure_resident && opt.precision == 64 && !opt.c_order) {
+    dw.s_inv = c->alloc<double>(static_cast<size_t>(W) * S * nqp * nn);
+    dw.s_pf = c->alloc<double>(static_cast<size_t>(W) * S * nqp);
+    dm.rinv = dw.s_inv;
+    dm.rpf = dw.s_pf;
+  }
   // measurement
   const size_t rows = static_cast<size_t>(W) * S;
   c->d_ostore = c->alloc<double>(rows * dm.sr_size);

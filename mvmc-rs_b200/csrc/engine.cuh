@@ -58,6 +58,10 @@ struct DevModel {
   const int* gone = nullptr;  // [ngone*4]: i, s, j, t of c†_{i s} c_{j t}
   const int* gtwo = nullptr;  // [ngtwo*8]: ri, rj, rk, rl, s, u, ref, gen
   const int* ggen = nullptr;  // [nggen*6]: ri, rj, rk, rl, s, u of the two-hop terms
+  // Resident measurement: each saved sample's Pf [nqp] and X⁻¹ [nqp][n][n] (FP64) as the
+  // sampler held them at the save point; null = recompute them from the configuration.
+  const double* rinv = nullptr;
+  const double* rpf = nullptr;
 };
 
 // Per-walker persistent state, arrays of W entries each.
@@ -85,6 +89,8 @@ struct DevWalkers {
   double* drift;              // [W] max |Δ ln|IP|| between the tracked and the refreshed amplitude
   long long* nrefresh;        // [W*2] scheduled (C rule / NRefresh) and guard-triggered refreshes
   double refresh_guard;       // refresh after an accepted move with a plane ratio outside [g, 1/g] (0 off)
+  double* s_inv = nullptr;    // [W*saved*nqp*n*n] FP64 X⁻¹ at each save point (resident measurement), or null
+  double* s_pf = nullptr;     // [W*saved*nqp] Pf at each save point
 };
 
 // One walker's Pfaffian stage buffers (device): FP64 planes and sweep scratch, Pf, the

@@ -427,21 +427,30 @@ __global__ void __launch_bounds__(NT, (kSmemPlane || NT > kMeasThreads ? 1 : 2))
       continue;
     }
     for (int q = 0; q < m.nqp; ++q) {
-      for (int k = tid; k < n * n; k += nt) {
-        const int i = k / n, j = k - i * n;
-        const int ri = idx[i] + (i >= ne ? ns : 0), rj = idx[j] + (j >= ne ? ns : 0);
-        A[k] = __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + ri) * m.ns2 + rj);
-      }
-      __syncthreads();
       double pfv;
       int st;
-      // planes in L2: a few rows in flight per warp, fewer for wide rows so that two
-      // samples share an SM
-      if (kSmemPlane)
-        gj_pfinv_pp<double, JPL, 1>(A, Bpp, n, pfv, st);
-      else  // in place: one plane per sample block in L2, rows p and q snapshot in shared memory
-        gj_pfinv_ip<double, JPL, (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, reinterpret_cast<double*>(smem + L.snap), n,
-                                                                       pfv, st);
+      if (m.rinv) {
+        // resident measurement: the sampler's Pf and X⁻¹ of this sample
+        const double* src = m.rinv + (static_cast<size_t>(sample) * m.nqp + q) * n * n;
+        for (int k = tid; k < n * n; k += nt) A[k] = src[k];
+        pfv = m.rpf[static_cast<size_t>(sample) * m.nqp + q];
+        st = 0;
+        __syncthreads();
+      } else {
+        for (int k = tid; k < n * n; k += nt) {
+          const int i = k / n, j = k - i * n;
+          const int ri = idx[i] + (i >= ne ? ns : 0), rj = idx[j] + (j >= ne ? ns : 0);
+          A[k] = __ldg(m.slater + (static_cast<size_t>(q) * m.ns2 + ri) * m.ns2 + rj);
+        }
+        __syncthreads();
+        // planes in L2: a few rows in flight per warp, fewer for wide rows so that two
+        // samples share an SM
+        if (kSmemPlane)
+          gj_pfinv_pp<double, JPL, 1>(A, Bpp, n, pfv, st);
+        else  // in place: one plane per sample block in L2, rows p and q snapshot in shared memory
+          gj_pfinv_ip<double, JPL, (JPL <= 2 ? 4 : (JPL <= 4 ? 2 : 1))>(A, reinterpret_cast<double*>(smem + L.snap),
+                                                                         n, pfv, st);
+      }
       if (st != 0) {
         if (tid == 0) s_bad = 1;
         __syncthreads();
@@ -699,15 +708,25 @@ __global__ void __launch_bounds__(kPackedThreads, 1)
       continue;
     }
     for (int q = 0; q < m.nqp; ++q) {
-      for (int i = warp; i < n - 1; i += nwarp) {  // X(i, j), i < j, from the Slater table
-        const int ri = idx[i] + (i >= ne ? ns : 0);
-        const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + ri) * m.ns2;
-        for (int j = i + 1 + lane; j < n; j += 32) P[rs[i] + j] = __ldg(srow + idx[j] + (j >= ne ? ns : 0));
-      }
-      __syncthreads();
       double pfv;
       int st;
-      gj_pfinv_packed<JPL, (kPackedThreads > 512 ? 1 : 2)>(P, rs, n, rowp, rowq, pfv, st);
+      if (m.rinv) {
+        // resident measurement: the upper triangle of the sampler's X⁻¹ of this sample
+        const double* src = m.rinv + (static_cast<size_t>(sample) * m.nqp + q) * n * n;
+        for (int i = warp; i < n - 1; i += nwarp)
+          for (int j = i + 1 + lane; j < n; j += 32) P[rs[i] + j] = src[static_cast<size_t>(i) * n + j];
+        pfv = m.rpf[static_cast<size_t>(sample) * m.nqp + q];
+        st = 0;
+        __syncthreads();
+      } else {
+        for (int i = warp; i < n - 1; i += nwarp) {  // X(i, j), i < j, from the Slater table
+          const int ri = idx[i] + (i >= ne ? ns : 0);
+          const double* srow = m.slater + (static_cast<size_t>(q) * m.ns2 + ri) * m.ns2;
+          for (int j = i + 1 + lane; j < n; j += 32) P[rs[i] + j] = __ldg(srow + idx[j] + (j >= ne ? ns : 0));
+        }
+        __syncthreads();
+        gj_pfinv_packed<JPL, (kPackedThreads > 512 ? 1 : 2)>(P, rs, n, rowp, rowq, pfv, st);
+      }
       if (st != 0) {
         if (tid == 0) s_bad = 1;
         __syncthreads();

@@ -1015,6 +1015,15 @@ __global__ void __launch_bounds__(NT, (SampOccupancy<NT, kSmemPlanes>::kBlocks))
         w.s_num[sample * m.ns2 + k] = s.num[k];
       }
       for (int k = tid; k < m.nproj; k += blockDim.x) w.s_cnt[sample * m.nproj + k] = s.cnt[k];
+      if constexpr (sizeof(T) == sizeof(double)) {
+        // resident measurement: this sample's Pf and X⁻¹ as the walker holds them
+        if (w.s_inv) {
+          const size_t nn = static_cast<size_t>(n) * n;
+          double* dst = w.s_inv + sample * m.nqp * nn;
+          for (size_t k = tid; k < m.nqp * nn; k += blockDim.x) dst[k] = s.planes[k];
+          for (int k = tid; k < m.nqp; k += blockDim.x) w.s_pf[sample * m.nqp + k] = s.pf[k];
+        }
+      }
     }
   }
   __syncthreads();

@@ -24,4 +24,5 @@ extern "C" void mvmc_b200_default_options(mvmc_b200_options* opt) {
   opt->refresh_guard = 0.0;
   opt->c_order = 0;
   opt->sr_gram = 0;
+  opt->measure_resident = 0;
 }

@@ -36,7 +36,8 @@ class Options(ctypes.Structure):
     _fields_ = [("walkers", ctypes.c_int), ("precision", ctypes.c_int),
                 ("refresh_sweeps", ctypes.c_int), ("saved_per_walker", ctypes.c_int),
                 ("seed", ctypes.c_longlong), ("device", ctypes.c_int), ("sr_precision", ctypes.c_int),
-                ("refresh_guard", ctypes.c_double), ("c_order", ctypes.c_int), ("sr_gram", ctypes.c_int)]
+                ("refresh_guard", ctypes.c_double), ("c_order", ctypes.c_int), ("sr_gram", ctypes.c_int),
+                ("measure_resident", ctypes.c_int)]
 
 
 def lib():

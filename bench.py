@@ -236,7 +236,8 @@ def time_engine(args, precision, W, namelist, initial_def, cfg, dims, rank, loca
     import mvmc_b200 as mb
     eng = mb.Engine(namelist, initial_def, walkers=W, precision=precision, seed=12345 + rank * W,
                     device=local, refresh_sweeps=args.refresh if precision == 32 else 0,
-                    refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision)
+                    refresh_guard=args.guard if precision == 32 else 0.0, sr_precision=sr_precision,
+                    sr_gram=1 if args.sr_gram else 0, measure_resident=1 if args.resident else 0)
     stream = torch.cuda.ExternalStream(eng.stream())
     energy = None
     if ws > 1:
@@ -572,6 +573,8 @@ def engine_bench(args, ws, rank, local):
                    "refresh_sweeps": args.refresh if args.precision == 32 else None,
                    "refresh_guard": args.guard if args.precision == 32 else None,
                    "sr_precision": args.sr_precision or 64, "sr": "direct" if args.direct else "cg",
+                   "sr_gram": bool(args.sr_gram),
+                   "measurement": "resident" if args.resident else "recomputed",
                    "l2": "inputs larger than L2 between steps (walker planes + O matrix)"},
         "sr_step_ms": main_rec["ms"] / args.steps, "sample_ms": main_rec["sample_ms"],
         "measure_ms": main_rec["measure_ms"], "energy": main_rec["energy"], "acceptance": p_acc,
@@ -942,6 +945,10 @@ def main():
     ap.add_argument("--sr-precision", type=int, default=0, choices=(0, 64, 32, 16),
                     help="SR operator storage of the timed engine (0: FP64)")
     ap.add_argument("--direct", action="store_true", help="direct SR (NSRCG 0): Gram + Cholesky instead of SR-CG")
+    ap.add_argument("--sr-gram", action="store_true",
+                    help="with --sr-precision 32/16: SR-CG through the tensor-core Gram of the samples")
+    ap.add_argument("--resident", action="store_true",
+                    help="FP64 path: measure from the sampler's resident Pf and inverse (not recomputed)")
     ap.add_argument("--no-extra", action="store_true",
                     help="square8: skip the 16x16 SR-step record, the Pfaffian records and the L2 ceiling")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

@@ -534,6 +534,137 @@ __global__ void __launch_bounds__(G * G, MB)
   }
 }
 
+// Uniform batches of side N ∈ {32, 64}, one warp per plane with no block barrier: the
+// plane lives in shared memory (row-major, the warp's own slice), lane l owns columns
+// l + 32c. A pivot step: every lane reads its columns of row p and the warp finds the
+// first maximum by shuffles; the lanes snapshot rows p and q (their own columns) into the
+// warp's two snapshot rows, and after a warp barrier update every row of their columns,
+// reading the row coefficients (row q and row p at the row's index) from the snapshots.
+// Same element formula and pivot rule as k_pfinv_reg / k_pfinv_uni.
+// Warps (planes) per block: FP64 planes of 64 take 34 KB each, so two per block and three
+// blocks fill an SM's shared memory.
+template <typename T, int N>
+struct PfWarps {
+  static constexpr int kPerBlock = (N == 64 && sizeof(T) == 8) ? 2 : 4;
+};
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * PfWarps<T, N>::kPerBlock)
+    k_pfinv_warp(const double* __restrict__ x, int planes, double* __restrict__ pf, double* __restrict__ inv,
+                 int* __restrict__ status) {
+  static_assert(N == 32 || N == 64, "one 64-bit swept mask, whole lanes per column set");
+  constexpr int C = N / 32, kPfWarpsPerBlock = PfWarps<T, N>::kPerBlock;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T* A = reinterpret_cast<T*>(smem) + static_cast<size_t>(warp) * (N * N + 2 * N);
+  T* SP = A + N * N;  // snapshot of row p
+  T* SQ = SP + N;     // snapshot of row q
+  const unsigned long long all = N == 64 ? ~0ull : ((1ull << N) - 1ull);
+  for (int plane = blockIdx.x * kPfWarpsPerBlock + warp; plane < planes; plane += gridDim.x * kPfWarpsPerBlock) {
+    const double* xp = x + static_cast<size_t>(plane) * N * N;
+    for (int k = lane; k < N * N; k += 32) A[k] = static_cast<T>(-xp[k]);
+    __syncwarp();
+    unsigned long long sw = 0ull;
+    int st = 0, parity = 0;
+    double pfv = 1.0;
+    for (int step = 0; step < N / 2; ++step) {
+      const unsigned long long free = ~sw & all;
+      const int p = __ffsll(static_cast<long long>(free)) - 1;
+      // pivot q: first maximum of |A(p, j)| over unswept j != p
+      double best = -1.0;
+      int bi = N;
+      T rp[C], rq[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int j = lane + 32 * c;
+        rp[c] = A[p * N + j];
+        if (j != p && !((sw >> j) & 1ull)) {
+          const double v = fabs(static_cast<double>(rp[c]));
+          if (v > best) {
+            best = v;
+            bi = j;
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (!(best > 0.0)) {
+        st = p + 1;
+        break;
+      }
+      const int q = bi;
+      const T a = A[p * N + q];
+      const T ia = T(1) / a;
+      pfv *= static_cast<double>(a);
+      {
+        const int len = q - p - 1;
+        if (len > 0) {
+          const unsigned long long range = (len == 64 ? ~0ull : ((1ull << len) - 1ull)) << (p + 1);
+          parity += __popcll(~sw & range);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int j = lane + 32 * c;
+        rq[c] = A[q * N + j];
+        SP[j] = rp[c];
+        SQ[j] = rq[c];
+      }
+      __syncwarp();
+#pragma unroll 4
+      for (int i = 0; i < N; ++i) {
+        const T rpi = SP[i], rqi = SQ[i];
+        const T ai = rqi * ia, bi2 = rpi * ia;
+        T* Ai = A + i * N;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int j = lane + 32 * c;
+          T v;
+          if (i == p) v = (j == q) ? -ia : (j == p ? T(0) : rq[c] * ia);
+          else if (i == q) v = (j == p) ? ia : (j == q ? T(0) : -rp[c] * ia);
+          else if (j == p) v = -rqi * ia;
+          else if (j == q) v = rpi * ia;
+          else v = Ai[j] + (ai * rp[c] - bi2 * rq[c]);
+          Ai[j] = v;
+        }
+      }
+      sw |= (1ull << p) | (1ull << q);
+      __syncwarp();
+    }
+    double* ip = inv + static_cast<size_t>(plane) * N * N;
+    for (int k = lane; k < N * N; k += 32) ip[k] = -static_cast<double>(A[k]);
+    if (lane == 0) {
+      double v = (parity & 1) ? -pfv : pfv;
+      if (st == 0 && !isfinite(v)) st = -1;
+      if (st != 0) v = 0.0;
+      pf[plane] = v;
+      status[plane] = st;
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T, int N>
+int launch_pfinv_warp(const double* x, int planes, double* pf, double* inv, int* status, cudaStream_t stream) {
+  constexpr int kPfWarpsPerBlock = PfWarps<T, N>::kPerBlock;
+  const size_t smem = sizeof(T) * kPfWarpsPerBlock * (static_cast<size_t>(N) * N + 2 * static_cast<size_t>(N));
+  auto kernel = k_pfinv_warp<T, N>;
+  MVMCB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 0;
+  MVMCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kPfWarpsPerBlock, smem));
+  const int blocks_needed = (planes + kPfWarpsPerBlock - 1) / kPfWarpsPerBlock;
+  const int grid = std::max(1, std::min(blocks_needed, std::max(1, per_sm) * device_sm_count()));
+  kernel<<<grid, 32 * kPfWarpsPerBlock, smem, stream>>>(x, planes, pf, inv, status);
+  MVMCB_CUDA(cudaGetLastError());
+  return kOk;
+}
+
 template <typename T, int N, int G, int MB>
 int launch_pfinv_uni(const double* x, int planes, double* pf, double* inv, int* status, cudaStream_t stream) {
   const size_t smem = sizeof(T) * (static_cast<size_t>(N) * (N + 1) + 6 * static_cast<size_t>(N));
@@ -686,15 +817,16 @@ int pfinv_device(const double* x, const int* sizes, const long long* offsets, in
   const int limit = device_smem_limit();
   if (!sizes && n_uniform == n_max && (n_max == 32 || n_max == 64) && (precision == 32 || precision == 64) &&
       !std::getenv("MVMC_B200_PFINV_TILE")) {
-    // uniform batches of 32 or 64: one barrier per pivot step (MVMC_B200_PFINV_TILE keeps
-    // the two-barrier tiles)
-    // (measured at B = 8192, n = 64: 1.31 ms FP64 / 1.03 ms FP32 against 1.49 / 1.16 ms for the
-    // two-barrier 16×4 tile; same bits; capping registers for two blocks per SM is slower)
-    if (precision == 32)
-      return n_max == 32 ? launch_pfinv_uni<float, 32, 16, 4>(x, planes, pf, inv, status, stream)
-                         : launch_pfinv_uni<float, 64, 16, 4>(x, planes, pf, inv, status, stream);
-    return n_max == 32 ? launch_pfinv_uni<double, 32, 16, 3>(x, planes, pf, inv, status, stream)
-                       : launch_pfinv_uni<double, 64, 16, 3>(x, planes, pf, inv, status, stream);
+    // uniform batches of 32 or 64 (MVMC_B200_PFINV_TILE keeps the two-barrier tiles), all
+    // with the same bits as those tiles. Side 32: one warp per plane, no block barrier
+    // (B = 8192: 0.24 ms FP64 / 0.17 ms FP32 against 0.46 / 0.37 ms for the two-barrier tile).
+    // Side 64: one barrier per pivot step (1.31 ms FP64 / 1.03 ms FP32 against 1.49 / 1.16 ms;
+    // a warp per plane holds a 34 KB FP64 plane, so only six fit an SM: 3.2 ms).
+    if (n_max == 32)
+      return precision == 32 ? launch_pfinv_warp<float, 32>(x, planes, pf, inv, status, stream)
+                             : launch_pfinv_warp<double, 32>(x, planes, pf, inv, status, stream);
+    if (precision == 32) return launch_pfinv_uni<float, 64, 16, 4>(x, planes, pf, inv, status, stream);
+    return launch_pfinv_uni<double, 64, 16, 3>(x, planes, pf, inv, status, stream);
   }
   if (n_max <= 128 && (precision == 32 || precision == 64)) {
     if (precision == 32)
